@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Benchmark: per-vertex triangle counting on one B200 (or N replicas).
+
+Default workload: R-MAT scale 20 (1,048,576 vertices), edge factor 16,
+(a,b,c,d) = (0.57, 0.19, 0.19, 0.05), seed 2; duplicates and self-loops
+removed, symmetrised, int64 offsets / int32 sorted adjacency; plain
+(per-vertex) mode: r, t, lcc and the global count.  A step is one complete
+count of the graph (all launches of one gtc_count call) with the CSR resident
+in HBM; L2 is flushed (a 256 MiB write) before every timed step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--config rmat20|er|rgg]
+
+Prints one JSON line.  Under torchrun (N > 1) every rank counts its own
+replica of the graph (no collective on the data path; "scaling": "weak") and
+the time is the max over ranks.  --impl reference times the reference's own
+CPU code (compiled from its sources into oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "per-vertex TC edges/s"
+UNIT = "undirected edges/s"
+L2_FLUSH_BYTES = 256 << 20
+
+CONFIGS = {
+    "rmat20": dict(kind="rmat", scale=20, ef=16, seed=2,
+                   label="R-MAT scale 20, edge factor 16, (0.57,0.19,0.19,0.05), seed 2"),
+    "er": dict(kind="er", n=16384, deg=16, seed=1,
+               label="Erdos-Renyi n=16384, mean degree 16, seed 1"),
+    "rgg": dict(kind="rgg", n=1 << 22, deg=12, seed=3,
+                label="2D RGG n=4194304, mean degree 12, Morton order, seed 3"),
+}
+
+
+def make_graph(cfg: dict, device):
+    from gputrianglecounting_b200 import graphs as G
+    if cfg["kind"] == "rmat":
+        return G.rmat(cfg["scale"], cfg["ef"], cfg["seed"], device=device)
+    if cfg["kind"] == "er":
+        return G.erdos_renyi(cfg["n"], cfg["deg"], cfg["seed"], device=device)
+    return G.rgg2d(cfg["n"], cfg["deg"], cfg["seed"], device=device)
+
+
+def algorithmic_bytes(host_graph) -> dict:
+    """B_alg = 4 W + 4 (n+1) + 4 nnz + 8 n + 8 n, W = sum over undirected
+    edges of min(d_u, d_v) (the per-unit work model of the hot path)."""
+    off = host_graph.off.astype(np.int64)
+    ind = host_graph.ind.astype(np.int64)
+    n = off.shape[0] - 1
+    deg = np.diff(off)
+    row = np.repeat(np.arange(n, dtype=np.int64), deg)
+    upper = row < ind
+    W = int(np.minimum(deg[row[upper]], deg[ind[upper]]).sum())
+    nnz = ind.shape[0]
+    return {"W": W, "B_alg": 4 * W + 4 * (n + 1) + 4 * nnz + 16 * n}
+
+
+def measured_peaks() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks / throttle reasons during timing."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.result = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.proc is None:
+            return False
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) != 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[2:]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if sm:
+            self.result = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                           "reasons": sorted(reasons), "samples": len(sm)}
+        return False
+
+
+# --------------------------------------------------------------- reference
+
+def reference_sample_rows(host_graph, stride: int, phase: int = 0) -> np.ndarray:
+    """Systematic sample of rows in degree order (every stride-th row), so the
+    sample holds its share of hub rows and low-degree rows alike."""
+    deg = np.diff(host_graph.off)
+    order = np.argsort(deg, kind="stable")
+    return np.ascontiguousarray(order[phase % stride::stride], dtype=np.int64)
+
+
+def time_reference_sample(prep, host_graph, stride, phase, threads):
+    from oracle import oracle as O
+    off64, ind64 = prep
+    rows = reference_sample_rows(host_graph, stride, phase)
+    tri = np.zeros(ind64.shape[0], np.int64)
+    r = np.zeros(off64.shape[0] - 1, np.int64)
+    t0 = time.perf_counter()
+    O.ref_rows_prepared(off64, ind64, rows, tri, r, threads)
+    dt = time.perf_counter() - t0
+    return dt, rows.shape[0]
+
+
+def calibrate_stride(prep, host_graph, threads, target_s: float) -> int:
+    """Pick the sampling stride so one sample takes about target_s seconds."""
+    n = host_graph.n
+    stride = max(1, n // 2000)
+    while True:
+        dt, _ = time_reference_sample(prep, host_graph, stride, 0, threads)
+        if dt > 0.2 or stride == 1:
+            break
+        stride = max(1, stride // 8)
+    est_full = dt * stride
+    return max(1, min(n, int(math.ceil(est_full / target_s)))), est_full
+
+
+def cpu_baseline(host_graph, threads: int, target_s: float = 4.0) -> dict:
+    from oracle import oracle as O
+    prep = O.ref_prepared(host_graph.off, host_graph.ind)
+    stride, _ = calibrate_stride(prep, host_graph, threads, target_s)
+    dt, rows = time_reference_sample(prep, host_graph, stride, 1, threads)
+    full = dt * stride
+    return {"value": host_graph.m / full, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"rows {rows} of {host_graph.n} (every {stride}-th row in degree order), "
+                      f"{dt:.2f} s; full-graph time estimated as sample x {stride} = {full:.1f} s"}
+
+
+def run_reference(args, cfg, rank: int) -> None:
+    import torch  # noqa: F401  (same environment as the GPU arm)
+    from oracle import oracle as O
+    if rank != 0:
+        return
+    g = make_graph(cfg, "cpu").numpy()
+    threads = O.max_threads()
+    prep = O.ref_prepared(g.off, g.ind)
+    stride, _ = calibrate_stride(prep, g, threads, 2.0)
+    for w in range(args.warmup):
+        time_reference_sample(prep, g, stride, w, threads)
+    est = []
+    rows_total = 0
+    for k in range(args.steps):
+        dt, rows = time_reference_sample(prep, g, stride, args.warmup + k, threads)
+        est.append(dt * stride)
+        rows_total += rows
+    full = statistics.mean(est)
+    value = g.m / full
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": full * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": args.config, "graph": cfg["label"], "n": g.n, "nnz": g.nnz,
+                   "m": g.m, "mode": "per-vertex (row sums of triNE)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"each step: every {stride}-th row in degree order "
+                                   f"(~{rows_total // max(1, args.steps)} rows) through the "
+                                   f"reference's count_all_trianglesCPU vertex-list overload, "
+                                   f"OpenMP dynamic,64; full-graph time = sample x {stride}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ b200
+
+def run_b200(args, cfg, rank: int, world: int) -> None:
+    import torch
+    import torch.distributed as dist
+    from gputrianglecounting_b200 import api
+    from gputrianglecounting_b200._lib import load as load_lib
+    load_lib()
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    # generated on the host (deterministic per seed, identical for both arms)
+    host = make_graph(cfg, "cpu").numpy()
+    g = host.to(dev)
+    torch.cuda.synchronize()
+    counter = api.TriangleCounter(dev)
+    out = None
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    # warm-up (also validates the input once)
+    reason, why = api.validate_csr(g.off, g.ind)
+    if reason != 0:
+        raise RuntimeError(f"generated graph invalid: {why}")
+    for _ in range(args.warmup):
+        out = counter.count(g.off, g.ind, out=out)
+    torch.cuda.synchronize()
+
+    # device-timed steps, one event pair per step, L2 flushed between steps
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)
+            evs[k][0].record(stream)
+            out = counter.count(g.off, g.ind, out=out)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    T = out.triangles
+
+    # phase breakdown of one count (events between the pipeline phases)
+    phases = phase_breakdown(counter, g, flush)
+
+    # end to end through the public API with host buffers (pinned), copies
+    # inside the timed region
+    h_off = torch.from_numpy(host.off).pin_memory()
+    h_ind = torch.from_numpy(host.ind).pin_memory()
+    h_r = torch.empty(host.n, dtype=torch.int64).pin_memory()
+    h_lcc = torch.empty(host.n, dtype=torch.float64).pin_memory()
+    h_glob = torch.empty(3, dtype=torch.int64).pin_memory()
+    d_off = torch.empty_like(g.off)
+    d_ind = torch.empty_like(g.ind)
+    e2e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+    for k in range(args.warmup + args.steps):
+        flush.fill_(k & 0xff)
+        if k >= args.warmup:
+            e2e_evs[k - args.warmup][0].record(stream)
+        d_off.copy_(h_off, non_blocking=True)
+        d_ind.copy_(h_ind, non_blocking=True)
+        res = counter.count(d_off, d_ind, outputs=("r", "lcc"))
+        h_r.copy_(res.r, non_blocking=True)
+        h_lcc.copy_(res.lcc, non_blocking=True)
+        h_glob.copy_(res.global_counts, non_blocking=True)
+        if k >= args.warmup:
+            e2e_evs[k - args.warmup][1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_evs)
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    assert int(h_glob[0]) == T, "end-to-end result differs from the device-resident run"
+    h2d = host.off.nbytes + host.ind.nbytes
+    d2h = h_r.numel() * 8 + h_lcc.numel() * 8 + 3 * 8
+
+    if rank != 0:
+        return
+    m = host.m
+    edges_all = m * world * args.steps
+    value = edges_all / (total_ms / 1e3)
+    ms_per_step = total_ms / args.steps
+    work = algorithmic_bytes(host)
+    peak, peak_kind = measured_peaks()
+    achieved = work["B_alg"] / (ms_per_step / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32 ids / int64 counts", "data": "synthetic",
+        "config": {"workload": args.config, "graph": cfg["label"], "n": host.n,
+                   "nnz": host.nnz, "m": m, "triangles": T, "mode": "plain (r, t, lcc, global)",
+                   "offsets": "int64", "l2": f"flushed before every timed step "
+                                               f"({L2_FLUSH_BYTES >> 20} MiB write)",
+                   "parallelism": f"{world} independent replica(s)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "scope": "one complete count (all launches of one gtc_count call)",
+                     "work_model": f"B_alg = 4W + 4(n+1) + 4nnz + 16n = {work['B_alg']} bytes, "
+                                   f"W = sum_undirected min(d_u, d_v) = {work['W']}",
+                     "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"},
+        "phases_ms": phases,
+        "e2e": {"value": m * world * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_ms / args.steps},
+        "clocks": clk.result,
+        "gpu_launches": LAUNCHES_PER_COUNT * args.steps,
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        line["cpu_baseline"] = cpu_baseline(host, O.max_threads())
+    print(json.dumps(line), flush=True)
+
+
+# degree, tile count, scan x3, tile fill, vinfo, scan x3, group kernel,
+# block kernel, finalize, global
+LAUNCHES_PER_COUNT = 14
+
+
+def phase_breakdown(counter, g, flush) -> dict:
+    """Per-phase device time of one count, from events the library records
+    between its phases (forward build / group kernel / block kernel /
+    epilogue), averaged over 3 runs."""
+    import ctypes
+
+    import torch
+    from gputrianglecounting_b200 import _lib
+    fn = _lib.load().gtc_count_phase_times
+    n, nnz = g.off.numel() - 1, g.ind.numel()
+    ws = counter._workspace(counter.workspace_bytes(n, nnz, 64))
+    res = []
+    for k in range(3):
+        flush.fill_(k)
+        times = (ctypes.c_float * 4)()
+        st = fn(g.off.data_ptr(), 64, g.ind.data_ptr(), n, nnz, ws.data_ptr(), ws.numel(),
+                ctypes.cast(times, ctypes.c_void_p))
+        _lib.check(st, "gtc_count_phase_times")
+        res.append(list(times))
+    torch.cuda.synchronize()
+    avg = [sum(r[i] for r in res) / len(res) for i in range(4)]
+    return {"forward_build": avg[0], "group_kernel": avg[1], "block_kernel": avg[2],
+            "epilogue": avg[3]}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="rmat20")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    cfg = CONFIGS[args.config]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, cfg, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_b200(args, cfg, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

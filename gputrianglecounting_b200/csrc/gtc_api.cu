@@ -1,0 +1,531 @@
+// gtc_api.cu -- the C ABI (include/gtc_b200.h): status strings, workspace
+// sizing, the counting entry points, the CSR validator, the vertex-subset
+// kernel and the reference-compatible kernelCall shims.
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "gtc_core.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace gtc {
+namespace {
+
+inline cudaStream_t as_stream(gtc_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ================================================================ validator
+
+// Phase 1: offsets start at 0, end at nnz, never decrease.
+template <typename OffT>
+__global__ void validate_offsets_kernel(const OffT *__restrict__ off, long long n,
+                                        long long nnz, int *reason)
+{
+    long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v == 0 && ((long long)off[0] != 0 || (long long)off[n] != nnz))
+        atomicMin(reason, GTC_CSR_BAD_OFFSETS);
+    if (v < n && (long long)off[v + 1] < (long long)off[v])
+        atomicMin(reason, GTC_CSR_BAD_OFFSETS);
+}
+
+// Phase 2 (warp per row): ids in range, no self-loop, strictly ascending.
+template <typename OffT>
+__global__ void validate_rows_kernel(const OffT *__restrict__ off,
+                                     const int *__restrict__ ind, long long n,
+                                     int *reason)
+{
+    if (*(volatile int *)reason != GTC_CSR_OK) return;
+    const int lane = threadIdx.x & 31;
+    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long a = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < n; a += warps) {
+        const long long rb = off[a], re = off[a + 1];
+        int bad = GTC_CSR_OK + 100;
+        for (long long e = rb + lane; e < re; e += 32) {
+            const int x = ind[e];
+            if ((unsigned long long)(long long)x >= (unsigned long long)n) bad = min(bad, (int)GTC_CSR_INDEX_RANGE);
+            else if (x == a) bad = min(bad, (int)GTC_CSR_SELF_LOOP);
+            if (e > rb && ind[e - 1] >= x) bad = min(bad, (int)GTC_CSR_UNSORTED_OR_DUPLICATE);
+        }
+        if (bad != GTC_CSR_OK + 100) atomicMin(reason, bad);
+    }
+}
+
+// Phase 3 (warp per row): every (a, x) has its mirror (x, a).
+template <typename OffT>
+__global__ void validate_symmetry_kernel(const OffT *__restrict__ off,
+                                         const int *__restrict__ ind, long long n,
+                                         int *reason)
+{
+    if (*(volatile int *)reason != GTC_CSR_OK) return;
+    const int lane = threadIdx.x & 31;
+    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long a = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < n; a += warps) {
+        const long long rb = off[a], re = off[a + 1];
+        bool ok = true;
+        for (long long e = rb + lane; e < re; e += 32) {
+            const int x = ind[e];
+            long long lo = off[x], hi = off[x + 1];
+            while (lo < hi) {
+                long long mid = (lo + hi) >> 1;
+                if (ind[mid] < a) lo = mid + 1; else hi = mid;
+            }
+            if (lo >= (long long)off[x + 1] || ind[lo] != a) ok = false;
+        }
+        if (!__all_sync(0xffffffffu, ok) && lane == 0) atomicMin(reason, GTC_CSR_ASYMMETRIC);
+    }
+}
+
+template <typename OffT>
+gtc_status run_validate(const OffT *off, const int *ind, long long n, long long nnz,
+                        void *ws, int32_t *h_reason, cudaStream_t stream)
+{
+    int *reason = static_cast<int *>(ws);
+    cudaError_t e = cudaMemsetAsync(reason, 0, sizeof(int), stream);
+    if (e != cudaSuccess) return GTC_ERR_CUDA;
+    const unsigned vb = (unsigned)div_up<long long>(n + 1, 256);
+    validate_offsets_kernel<<<vb, 256, 0, stream>>>(off, n, nnz, reason);
+    if (n > 0) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        long long want = div_up<long long>(n, 8);
+        unsigned blocks = (unsigned)(want < (long long)sms * 16 ? want : (long long)sms * 16);
+        validate_rows_kernel<<<blocks, 256, 0, stream>>>(off, ind, n, reason);
+        validate_symmetry_kernel<<<blocks, 256, 0, stream>>>(off, ind, n, reason);
+    }
+    int host = 0;
+    e = cudaMemcpyAsync(&host, reason, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e != cudaSuccess) return GTC_ERR_CUDA;
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return GTC_ERR_CUDA;
+    *h_reason = host;
+    return GTC_OK;
+}
+
+// ============================================================ vertex subset
+
+constexpr int kSubThreads = 256;
+constexpr int kSubSlots = 4096;
+
+template <typename IndT>
+__device__ __forceinline__ bool sorted_contains(const IndT *__restrict__ list,
+                                                long long len, long long key)
+{
+    long long lo = 0, hi = len;
+    while (lo < hi) {
+        long long mid = (lo + hi) >> 1;
+        if ((long long)list[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    return lo < len && (long long)list[lo] == key;
+}
+
+// out[k] = sum over u in N(v) of |N(v) ∩ N(u)|, v = vertex[k], with full
+// adjacency lists (the rows of the listed vertices and of their neighbours
+// are the only ones read, as in the reference's vertex-list kernel,
+// src/clusteringCount.cu:266-312).  Block per listed vertex: N(v) goes to a
+// shared hash table; for each neighbour u the shorter side is probed (N(u)
+// into the table, or N(v) by binary search into N(u)).  Edges with u == v
+// or a list shorter than two are skipped like the reference (:292-294).
+template <typename OffT, typename IndT, typename VtxT, typename OutT>
+__global__ void __launch_bounds__(kSubThreads)
+subset_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
+              const VtxT *__restrict__ vertex, long long count,
+              OutT *__restrict__ out)
+{
+    __shared__ long long s_keys[kSubSlots];
+    __shared__ unsigned long long s_sum;
+    auto block = cg::this_thread_block();
+    auto warp = cg::tiled_partition<32>(block);
+    const int wid = warp.meta_group_rank(), lane = warp.thread_rank();
+    constexpr int nwarps = kSubThreads / 32;
+    for (long long k = blockIdx.x; k < count; k += gridDim.x) {
+        const long long v = (long long)vertex[k];
+        const long long vb = off[v], ve = off[v + 1], dv = ve - vb;
+        if (threadIdx.x == 0) s_sum = 0;
+        const bool use_table = dv <= kSubSlots / 2;
+        int log2t = 5;
+        while ((1ll << log2t) < 2 * dv) ++log2t;
+        const unsigned int mask = (1u << log2t) - 1;
+        if (use_table) {
+            for (int i = threadIdx.x; i <= (int)mask; i += kSubThreads) s_keys[i] = -1;
+            __syncthreads();
+            for (long long i = threadIdx.x; i < dv; i += kSubThreads) {
+                const long long key = (long long)ind[vb + i];
+                unsigned int slot = hash_slot((int)key, log2t);
+                while (true) {
+                    unsigned long long prev = atomicCAS((unsigned long long *)&s_keys[slot],
+                                                        (unsigned long long)-1ll,
+                                                        (unsigned long long)key);
+                    if (prev == (unsigned long long)-1ll) break;
+                    slot = (slot + 1) & mask;
+                }
+            }
+        }
+        __syncthreads();
+        unsigned long long acc = 0;
+        if (dv >= 2) {
+            // warps take neighbours u in turn
+            for (long long e = vb + wid; e < ve; e += nwarps) {
+                const long long u = (long long)ind[e];
+                const long long ub = off[u], ue = off[u + 1], du = ue - ub;
+                if (u == v || du < 2) continue;
+                if (use_table && du <= 4 * dv) {
+                    for (long long i = lane; i < du; i += 32) {
+                        const long long w = (long long)ind[ub + i];
+                        unsigned int slot = hash_slot((int)w, log2t);
+                        while (true) {
+                            const long long kk = s_keys[slot];
+                            if (kk == w) { ++acc; break; }
+                            if (kk == -1) break;
+                            slot = (slot + 1) & mask;
+                        }
+                    }
+                } else {
+                    for (long long i = lane; i < dv; i += 32) {
+                        const long long w = (long long)ind[vb + i];
+                        acc += sorted_contains(ind + ub, du, w);
+                    }
+                }
+            }
+        }
+        const unsigned long long ws = cg::reduce(warp, acc, cg::plus<unsigned long long>());
+        if (lane == 0 && ws) atomicAdd(&s_sum, ws);
+        __syncthreads();
+        if (threadIdx.x == 0) out[k] = (OutT)s_sum;
+        __syncthreads();
+    }
+}
+
+template <typename OffT, typename IndT, typename VtxT, typename OutT>
+gtc_status launch_subset(const OffT *off, const IndT *ind, const VtxT *vertex,
+                         long long count, OutT *out, cudaStream_t stream)
+{
+    if (count <= 0) return GTC_OK;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long long blocks = count < (long long)sms * 8 ? count : (long long)sms * 8;
+    subset_kernel<OffT, IndT, VtxT, OutT><<<(unsigned)blocks, kSubThreads, 0, stream>>>(
+        off, ind, vertex, count, out);
+    return cudaGetLastError() == cudaSuccess ? GTC_OK : GTC_ERR_CUDA;
+}
+
+// ================================================================== compat
+
+__global__ void narrow_kernel(const long long *__restrict__ in, int *__restrict__ out,
+                              long long count)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) out[i] = (int)in[i];
+}
+
+__global__ void narrow_out_kernel(const long long *__restrict__ in, int *__restrict__ out,
+                                  long long count)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) out[i] = (int)in[i];
+}
+
+struct CompatCache {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+std::mutex g_compat_mu;
+CompatCache g_compat[64];
+thread_local gtc_status g_compat_status = GTC_OK;
+
+void *compat_workspace(size_t bytes)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_compat_mu);
+    CompatCache &c = g_compat[dev];
+    if (c.bytes < bytes) {
+        if (c.ptr) cudaFree(c.ptr);
+        c.ptr = nullptr;
+        c.bytes = 0;
+        if (cudaMalloc(&c.ptr, bytes) != cudaSuccess) { c.ptr = nullptr; return nullptr; }
+        c.bytes = bytes;
+    }
+    return c.ptr;
+}
+
+bool compat_block_size_ok(unsigned int bs)
+{
+    switch (bs) {
+    case 32: case 64: case 96: case 128: case 192: case 256: case 512: case 1024: return true;
+    default: return false;
+    }
+}
+
+}  // namespace
+}  // namespace gtc
+
+using namespace gtc;
+
+extern "C" {
+
+const char *gtc_status_string(gtc_status s)
+{
+    switch (s) {
+    case GTC_OK: return "ok";
+    case GTC_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case GTC_ERR_INVALID_CSR: return "invalid CSR";
+    case GTC_ERR_WORKSPACE_TOO_SMALL: return "workspace too small";
+    case GTC_ERR_CUDA: return "CUDA runtime error";
+    case GTC_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case GTC_ERR_UNSUPPORTED: return "unsupported device or configuration";
+    case GTC_ERR_TIMEOUT: return "bounded device wait timed out";
+    case GTC_ERR_CAPACITY: return "capacity exceeded";
+    case GTC_ERR_BUSY: return "busy";
+    }
+    return "unknown status";
+}
+
+gtc_status gtc_device_info(int *sm_count, int *cc)
+{
+    if (!sm_count || !cc) return GTC_ERR_INVALID_ARGUMENT;
+    int dev = 0, major = 0, minor = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GTC_ERR_CUDA;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev) != cudaSuccess)
+        return GTC_ERR_CUDA;
+    *sm_count = sms;
+    *cc = major * 10 + minor;
+    return GTC_OK;
+}
+
+gtc_status gtc_workspace_size(int64_t n, int64_t nnz, int off_bits, gtc_mode mode, size_t *bytes)
+{
+    if (!bytes || n < 0 || nnz < 0 || (off_bits != 32 && off_bits != 64)) return GTC_ERR_INVALID_ARGUMENT;
+    if (mode != GTC_MODE_PLAIN && mode != GTC_MODE_ORIENTED) return GTC_ERR_INVALID_ARGUMENT;
+    if (n > 0x7fffffffll) return GTC_ERR_UNSUPPORTED;           // int32 vertex ids
+    if (off_bits == 32 && nnz > 0x7fffffffll) return GTC_ERR_INVALID_ARGUMENT;
+    *bytes = make_plan(n, nnz, off_bits, mode == GTC_MODE_PLAIN).bytes;
+    return GTC_OK;
+}
+
+gtc_status gtc_count_tuned(const void *d_off, int off_bits, const int32_t *d_ind, int64_t n,
+                           int64_t nnz, gtc_mode mode, int64_t *d_r, int64_t *d_t,
+                           double *d_lcc, int64_t *d_global, void *d_workspace, size_t ws_bytes,
+                           gtc_stream_t stream, const gtc_tuning *tuning)
+{
+    size_t need = 0;
+    gtc_status st = gtc_workspace_size(n, nnz, off_bits, mode, &need);
+    if (st != GTC_OK) return st;
+    if (!d_off || (nnz > 0 && !d_ind) || !d_workspace) return GTC_ERR_INVALID_ARGUMENT;
+    if (mode == GTC_MODE_ORIENTED && (d_r || d_t || d_lcc)) return GTC_ERR_INVALID_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(d_workspace) & 255) return GTC_ERR_INVALID_ARGUMENT;
+    if (ws_bytes < need) return GTC_ERR_WORKSPACE_TOO_SMALL;
+    const bool pv = mode == GTC_MODE_PLAIN;
+    RowConfig cfg = pick_row_config(n, nnz);
+    if (tuning) {
+        if (tuning->group) {
+            if (tuning->group != 4 && tuning->group != 8 && tuning->group != 16 &&
+                tuning->group != 32)
+                return GTC_ERR_INVALID_ARGUMENT;
+            cfg.group = tuning->group;
+        }
+        if (tuning->item_len < 0 || tuning->big_chunk < 0 || tuning->big_hash_max < 0 ||
+            tuning->big_hash_max > kBigHashMaxFdeg)
+            return GTC_ERR_INVALID_ARGUMENT;
+        if (tuning->item_len) cfg.item_len = tuning->item_len;
+        if (tuning->big_chunk) cfg.big_chunk = tuning->big_chunk;
+        if (tuning->big_hash_max) cfg.big_hash_max = tuning->big_hash_max;
+    }
+    long long *r = reinterpret_cast<long long *>(d_r);
+    long long *t = reinterpret_cast<long long *>(d_t);
+    long long *g = reinterpret_cast<long long *>(d_global);
+    if (off_bits == 32)
+        return run_count<int>(static_cast<const int *>(d_off), d_ind, n, nnz, pv, r, t, d_lcc, g,
+                              d_workspace, ws_bytes, as_stream(stream), cfg, nullptr);
+    return run_count<long long>(static_cast<const long long *>(d_off), d_ind, n, nnz, pv, r, t,
+                                d_lcc, g, d_workspace, ws_bytes, as_stream(stream), cfg, nullptr);
+}
+
+gtc_status gtc_count(const void *d_off, int off_bits, const int32_t *d_ind, int64_t n,
+                     int64_t nnz, gtc_mode mode, int64_t *d_r, int64_t *d_t, double *d_lcc,
+                     int64_t *d_global, void *d_workspace, size_t ws_bytes, gtc_stream_t stream)
+{
+    return gtc_count_tuned(d_off, off_bits, d_ind, n, nnz, mode, d_r, d_t, d_lcc, d_global,
+                           d_workspace, ws_bytes, stream, nullptr);
+}
+
+gtc_status gtc_count_phase_times(const void *d_off, int off_bits, const int32_t *d_ind,
+                                 int64_t n, int64_t nnz, void *d_workspace, size_t ws_bytes,
+                                 float *h_ms)
+{
+    size_t need = 0;
+    gtc_status st = gtc_workspace_size(n, nnz, off_bits, GTC_MODE_PLAIN, &need);
+    if (st != GTC_OK) return st;
+    if (!d_off || (nnz > 0 && !d_ind) || !d_workspace || !h_ms) return GTC_ERR_INVALID_ARGUMENT;
+    if (ws_bytes < need) return GTC_ERR_WORKSPACE_TOO_SMALL;
+    CountTimings tm;
+    for (int i = 0; i < 5; ++i)
+        if (cudaEventCreate(&tm.ev[i]) != cudaSuccess) return GTC_ERR_CUDA;
+    RowConfig cfg = pick_row_config(n, nnz);
+    if (off_bits == 32)
+        st = run_count<int>(static_cast<const int *>(d_off), d_ind, n, nnz, true, nullptr,
+                            nullptr, nullptr, nullptr, d_workspace, ws_bytes, 0, cfg, &tm);
+    else
+        st = run_count<long long>(static_cast<const long long *>(d_off), d_ind, n, nnz, true,
+                                  nullptr, nullptr, nullptr, nullptr, d_workspace, ws_bytes, 0,
+                                  cfg, &tm);
+    if (st == GTC_OK && cudaEventSynchronize(tm.ev[4]) != cudaSuccess) st = GTC_ERR_CUDA;
+    if (st == GTC_OK && n > 0) {
+        for (int i = 0; i < 4; ++i) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, tm.ev[i], tm.ev[i + 1]);
+            h_ms[i] = ms;
+        }
+    }
+    for (int i = 0; i < 5; ++i) cudaEventDestroy(tm.ev[i]);
+    return st;
+}
+
+size_t gtc_validate_workspace_size(int64_t n, int64_t nnz)
+{
+    (void)n;
+    (void)nnz;
+    return 256;
+}
+
+gtc_status gtc_validate_csr(const void *d_off, int off_bits, const int32_t *d_ind, int64_t n,
+                            int64_t nnz, void *d_workspace, size_t ws_bytes, int32_t *h_reason,
+                            gtc_stream_t stream)
+{
+    if (!d_off || (nnz > 0 && !d_ind) || !d_workspace || !h_reason || n < 0 || nnz < 0)
+        return GTC_ERR_INVALID_ARGUMENT;
+    if (off_bits != 32 && off_bits != 64) return GTC_ERR_INVALID_ARGUMENT;
+    if (n > 0x7fffffffll) return GTC_ERR_UNSUPPORTED;
+    if (ws_bytes < gtc_validate_workspace_size(n, nnz)) return GTC_ERR_WORKSPACE_TOO_SMALL;
+    if (off_bits == 32)
+        return run_validate<int>(static_cast<const int *>(d_off), d_ind, n, nnz, d_workspace,
+                                 h_reason, as_stream(stream));
+    return run_validate<long long>(static_cast<const long long *>(d_off), d_ind, n, nnz,
+                                   d_workspace, h_reason, as_stream(stream));
+}
+
+gtc_status gtc_count_subset(const void *d_off, int off_bits, const int32_t *d_ind,
+                            const int32_t *d_vertex, int64_t count, int64_t *d_out,
+                            gtc_stream_t stream)
+{
+    if (count < 0) return GTC_ERR_INVALID_ARGUMENT;
+    if (count == 0) return GTC_OK;
+    if (!d_off || !d_ind || !d_vertex || !d_out) return GTC_ERR_INVALID_ARGUMENT;
+    if (off_bits == 32)
+        return launch_subset(static_cast<const int *>(d_off), d_ind, d_vertex, count,
+                             reinterpret_cast<long long *>(d_out), as_stream(stream));
+    if (off_bits == 64)
+        return launch_subset(static_cast<const long long *>(d_off), d_ind, d_vertex, count,
+                             reinterpret_cast<long long *>(d_out), as_stream(stream));
+    return GTC_ERR_INVALID_ARGUMENT;
+}
+
+gtc_status gtc_compat_last_status(void) { return g_compat_status; }
+
+gtc_status gtc_compat_release(void)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return GTC_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_compat_mu);
+    CompatCache &c = g_compat[dev];
+    if (c.ptr) cudaFree(c.ptr);
+    c.ptr = nullptr;
+    c.bytes = 0;
+    return GTC_OK;
+}
+
+void gtc_kernelCall_i64(unsigned int numberBlocks, unsigned int numberThreads, int64_t nv,
+                        const int64_t *d_off, const int64_t *d_ind, int64_t *out,
+                        int64_t threads_per_block, int64_t number_blocks, int64_t shifter)
+{
+    (void)numberBlocks; (void)threads_per_block; (void)number_blocks; (void)shifter;
+    g_compat_status = GTC_OK;
+    if (!compat_block_size_ok(numberThreads)) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
+    if (nv <= 0 || !d_off || !out) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
+    int64_t nnz = 0;
+    // the pipeline needs nnz = off[nv]: one 8-byte read on the legacy stream
+    if (cudaMemcpy(&nnz, d_off + nv, sizeof(int64_t), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        g_compat_status = GTC_ERR_CUDA;
+        return;
+    }
+    if (nnz < 0 || nv > 0x7fffffffll) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
+    size_t need = make_plan(nv, nnz, 64, true).bytes;
+    size_t ind_bytes = (((size_t)nnz * sizeof(int)) + 255) & ~(size_t)255;
+    char *ws = static_cast<char *>(compat_workspace(need + ind_bytes));
+    if (!ws) { g_compat_status = GTC_ERR_OUT_OF_MEMORY; return; }
+    int *ind32 = reinterpret_cast<int *>(ws + need);
+    if (nnz > 0)
+        narrow_kernel<<<(unsigned)div_up<long long>(nnz, 256), 256>>>(
+            reinterpret_cast<const long long *>(d_ind), ind32, nnz);
+    RowConfig cfg = pick_row_config(nv, nnz);
+    g_compat_status = run_count<long long>(reinterpret_cast<const long long *>(d_off), ind32, nv,
+                                           nnz, true, reinterpret_cast<long long *>(out), nullptr,
+                                           nullptr, nullptr, ws, need, 0, cfg, nullptr);
+}
+
+void gtc_kernelCall_i32(unsigned int numberBlocks, unsigned int numberThreads, int32_t nv,
+                        const int32_t *d_off, const int32_t *d_ind, int32_t *out,
+                        int32_t threads_per_block, int32_t number_blocks, int32_t shifter)
+{
+    (void)numberBlocks; (void)threads_per_block; (void)number_blocks; (void)shifter;
+    g_compat_status = GTC_OK;
+    if (!compat_block_size_ok(numberThreads)) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
+    if (nv <= 0 || !d_off || !out) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
+    int32_t nnz = 0;
+    if (cudaMemcpy(&nnz, d_off + nv, sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        g_compat_status = GTC_ERR_CUDA;
+        return;
+    }
+    if (nnz < 0) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
+    size_t need = make_plan(nv, nnz, 32, true).bytes;
+    size_t r_bytes = (((size_t)nv * sizeof(long long)) + 255) & ~(size_t)255;
+    char *ws = static_cast<char *>(compat_workspace(need + r_bytes));
+    if (!ws) { g_compat_status = GTC_ERR_OUT_OF_MEMORY; return; }
+    long long *r64 = reinterpret_cast<long long *>(ws + need);
+    RowConfig cfg = pick_row_config(nv, nnz);
+    g_compat_status = run_count<int>(d_off, d_ind, nv, nnz, true, r64, nullptr, nullptr, nullptr,
+                                     ws, need, 0, cfg, nullptr);
+    if (g_compat_status == GTC_OK)
+        narrow_out_kernel<<<(unsigned)div_up<long long>(nv, 256), 256>>>(r64, out, nv);
+}
+
+void gtc_kernelCall_vertex_i64(unsigned int numberBlocks, unsigned int numberThreads, int64_t nv,
+                               const int64_t *vertex, const int64_t *d_off, const int64_t *d_ind,
+                               int64_t *out, int64_t threads_per_block, int64_t number_blocks,
+                               int64_t shifter)
+{
+    (void)numberBlocks; (void)threads_per_block; (void)number_blocks; (void)shifter;
+    g_compat_status = GTC_OK;
+    if (!compat_block_size_ok(numberThreads)) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
+    if (nv < 0 || (nv > 0 && (!vertex || !d_off || !d_ind || !out))) {
+        g_compat_status = GTC_ERR_INVALID_ARGUMENT;
+        return;
+    }
+    g_compat_status = launch_subset(reinterpret_cast<const long long *>(d_off),
+                                    reinterpret_cast<const long long *>(d_ind),
+                                    reinterpret_cast<const long long *>(vertex), nv,
+                                    reinterpret_cast<long long *>(out), 0);
+}
+
+void gtc_kernelCall_vertex_i32(unsigned int numberBlocks, unsigned int numberThreads, int32_t nv,
+                               const int32_t *vertex, const int32_t *d_off, const int32_t *d_ind,
+                               int32_t *out, int32_t threads_per_block, int32_t number_blocks,
+                               int32_t shifter)
+{
+    (void)numberBlocks; (void)threads_per_block; (void)number_blocks; (void)shifter;
+    g_compat_status = GTC_OK;
+    if (!compat_block_size_ok(numberThreads)) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
+    if (nv < 0 || (nv > 0 && (!vertex || !d_off || !d_ind || !out))) {
+        g_compat_status = GTC_ERR_INVALID_ARGUMENT;
+        return;
+    }
+    g_compat_status = launch_subset(d_off, d_ind, vertex, (long long)nv, out, 0);
+}
+
+}  // extern "C"

@@ -1,0 +1,714 @@
+// gtc_core.cu -- the single-graph counting pipeline: forward-list build
+// (merge-path tiles over rows + entries), apex/partner intersection kernels
+// and the exact epilogue (r = 2t, lcc, global count).
+//
+// Reference operator replaced: count_all_trianglesGPU<T,bs> + kernelCall<T>
+// (src/clusteringCount.cu:314-359, :415-467) and the thrust::reduce global
+// sum (src/gpurun.cu:40).
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+#include <cooperative_groups/scan.h>
+
+#include "gtc_core.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace gtc {
+
+// ======================================================= forward-list build
+
+__global__ void degree_kernel(const void *off_v, int off_bits, long long n,
+                              int *__restrict__ deg)
+{
+    long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    if (off_bits == 32) {
+        const int *off = static_cast<const int *>(off_v);
+        deg[v] = off[v + 1] - off[v];
+    } else {
+        const long long *off = static_cast<const long long *>(off_v);
+        deg[v] = (int)(off[v + 1] - off[v]);
+    }
+}
+
+// Rows consumed at merge-path diagonal `diag` of the merge of the row-end
+// offsets off[1..n] with the entry indices 0..nnz-1 (Merrill & Garland,
+// "Merge-based parallel sparse matrix-vector multiplication", SC'16).
+template <typename OffT>
+__device__ __forceinline__ long long mp_rows(const OffT *__restrict__ off,
+                                             long long n, long long nnz,
+                                             long long diag)
+{
+    long long lo = diag - nnz > 0 ? diag - nnz : 0;
+    long long hi = diag < n ? diag : n;
+    while (lo < hi) {
+        long long mid = (lo + hi) >> 1;
+        if ((long long)off[mid + 1] <= diag - mid - 1) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Shared state of one merge-path tile: rows r0..r1 (offsets staged from
+// off[r0]) and entries e0..e1 (adjacency staged).
+struct TileSmem {
+    long long off[kPrepTile + 2];
+    int ind[kPrepTile];
+    long long r0, e0, r1, e1;
+};
+
+template <typename OffT>
+__device__ void tile_stage(TileSmem &s, const OffT *__restrict__ off,
+                           const int *__restrict__ ind, long long n,
+                           long long nnz)
+{
+    long long d0 = (long long)blockIdx.x * kPrepTile;
+    long long d1 = d0 + kPrepTile;
+    if (d1 > n + nnz) d1 = n + nnz;
+    if (threadIdx.x == 0) {
+        long long r = mp_rows(off, n, nnz, d0);
+        s.r0 = r; s.e0 = d0 - r;
+    } else if (threadIdx.x == 32) {
+        long long r = mp_rows(off, n, nnz, d1);
+        s.r1 = r; s.e1 = d1 - r;
+    }
+    __syncthreads();
+    const long long r0 = s.r0, r1 = s.r1, e0 = s.e0, e1 = s.e1;
+    // off[r0 .. r1+1], clamped to off[n]
+    for (long long k = threadIdx.x; k <= r1 - r0 + 1; k += blockDim.x) {
+        long long r = r0 + k;
+        s.off[k] = (long long)off[r <= n ? r : n];
+    }
+    for (long long k = threadIdx.x; k < e1 - e0; k += blockDim.x)
+        s.ind[k] = ind[e0 + k];
+    __syncthreads();
+}
+
+// Local merge-path start of this thread inside the staged tile.
+__device__ __forceinline__ void tile_thread_start(const TileSmem &s,
+                                                  long long &li, long long &lj)
+{
+    const long long rows = s.r1 - s.r0, ents = s.e1 - s.e0;
+    long long ld = (long long)threadIdx.x * kPrepItemsPerThread;
+    if (ld > rows + ents) ld = rows + ents;
+    long long lo = ld - ents > 0 ? ld - ents : 0;
+    long long hi = ld < rows ? ld : rows;
+    while (lo < hi) {
+        long long mid = (lo + hi) >> 1;
+        if (s.off[mid + 1] - s.e0 <= ld - mid - 1) lo = mid + 1; else hi = mid;
+    }
+    li = lo;
+    lj = ld - lo;
+}
+
+// Forward flag of the entry at local (li, lj): does ind[e] outrank the row?
+__device__ __forceinline__ bool entry_forward(const TileSmem &s, long long li,
+                                              long long lj,
+                                              const int *__restrict__ deg,
+                                              long long n,
+                                              unsigned int *status)
+{
+    const long long a = s.r0 + li;
+    const int da = (int)(s.off[li + 1] - s.off[li]);
+    const int x = s.ind[lj];
+    if ((unsigned long long)(long long)x >= (unsigned long long)n) {
+        atomicOr(status, kErrIndexRange);
+        return false;
+    }
+    return rank_above(deg[x], x, da, (int)a);
+}
+
+// Pass 1: number of forward entries per tile.
+template <typename OffT>
+__global__ void __launch_bounds__(kPrepThreads)
+tile_count_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
+                  const int *__restrict__ deg, long long n, long long nnz,
+                  long long *__restrict__ tile_cnt, unsigned int *status)
+{
+    __shared__ TileSmem s;
+    tile_stage(s, off, ind, n, nnz);
+    long long li, lj;
+    tile_thread_start(s, li, lj);
+    const long long rows = s.r1 - s.r0, ents = s.e1 - s.e0;
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < kPrepItemsPerThread; ++k) {
+        if (li + lj >= rows + ents) break;
+        if (li < rows && lj >= s.off[li + 1] - s.e0) {
+            ++li;                                   // row end
+        } else {
+            cnt += entry_forward(s, li, lj, deg, n, status);
+            ++lj;
+        }
+    }
+    __shared__ int warp_sum[kPrepThreads / 32];
+    int w = cnt;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = w;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long t = 0;
+        for (int i = 0; i < kPrepThreads / 32; ++i) t += warp_sum[i];
+        tile_cnt[blockIdx.x] = t;
+    }
+}
+
+// Pass 2: write the forward adjacency (ordered stream compaction of the
+// adjacency by the forward flag) and the forward offsets foff[r+1] at every
+// row end.
+template <typename OffT>
+__global__ void __launch_bounds__(kPrepThreads)
+tile_fill_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
+                 const int *__restrict__ deg, long long n, long long nnz,
+                 const long long *__restrict__ tile_pre,
+                 long long *__restrict__ foff, int *__restrict__ find,
+                 unsigned int *status)
+{
+    __shared__ TileSmem s;
+    __shared__ int warp_sum[kPrepThreads / 32];
+    tile_stage(s, off, ind, n, nnz);
+    long long li, lj;
+    tile_thread_start(s, li, lj);
+    const long long li0 = li, lj0 = lj;
+    const long long rows = s.r1 - s.r0, ents = s.e1 - s.e0;
+    unsigned int flags = 0;
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < kPrepItemsPerThread; ++k) {
+        if (li + lj >= rows + ents) break;
+        if (li < rows && lj >= s.off[li + 1] - s.e0) {
+            ++li;
+        } else {
+            if (entry_forward(s, li, lj, deg, n, status)) { flags |= 1u << k; ++cnt; }
+            ++lj;
+        }
+    }
+    // block exclusive scan of cnt
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        int o = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += o;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    int wbase = 0;
+    for (int i = 0; i < warp; ++i) wbase += warp_sum[i];
+    long long pos = tile_pre[blockIdx.x] + wbase + incl - cnt;
+    if (blockIdx.x == 0 && threadIdx.x == 0) foff[0] = 0;
+    li = li0; lj = lj0;
+#pragma unroll
+    for (int k = 0; k < kPrepItemsPerThread; ++k) {
+        if (li + lj >= rows + ents) break;
+        if (li < rows && lj >= s.off[li + 1] - s.e0) {
+            foff[s.r0 + li + 1] = pos;              // row r0+li ends here
+            ++li;
+        } else {
+            if (flags & (1u << k)) find[pos++] = s.ind[lj];
+            ++lj;
+        }
+    }
+}
+
+// Per-vertex record and block-kernel work: rows whose forward list exceeds
+// the group kernel's table get ceil(deg / big_chunk) block items.
+__global__ void vinfo_kernel(const long long *__restrict__ foff,
+                             const int *__restrict__ deg, long long n,
+                             int small_cap, int big_chunk,
+                             VInfo *__restrict__ vinfo,
+                             long long *__restrict__ big_items)
+{
+    long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    VInfo r;
+    r.fbeg = foff[v];
+    r.fdeg = (int)(foff[v + 1] - r.fbeg);
+    r.deg = deg[v];
+    vinfo[v] = r;
+    big_items[v] = (r.fdeg > small_cap) ? div_up<long long>(r.deg, big_chunk) : 0;
+}
+
+// ============================================================ intersection
+
+// Shared-memory open-addressing table of one apex's forward list.
+struct ApexTable {
+    int *keys;
+    int *hits;
+    int log2_slots;
+    unsigned int mask;
+
+    __device__ __forceinline__ void insert(int key) const
+    {
+        unsigned int slot = hash_slot(key, log2_slots);
+        while (true) {
+            int prev = atomicCAS(&keys[slot], -1, key);
+            if (prev == -1) return;
+            slot = (slot + 1) & mask;
+        }
+    }
+    __device__ __forceinline__ int find(int key) const
+    {
+        unsigned int slot = hash_slot(key, log2_slots);
+        while (true) {
+            int k = keys[slot];
+            if (k == key) return (int)slot;
+            if (k == -1) return -1;
+            slot = (slot + 1) & mask;
+        }
+    }
+};
+
+// Binary search of a sorted global forward list (block kernel, apexes whose
+// forward list is larger than the shared table).
+__device__ __forceinline__ int sorted_find(const int *__restrict__ list,
+                                           int len, int key)
+{
+    int lo = 0, hi = len;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        int v = list[mid];
+        if (v < key) lo = mid + 1; else hi = mid;
+    }
+    return (lo < len && list[lo] == key) ? lo : -1;
+}
+
+// One stride of up to G adjacency entries of apex `a` (entries s..s+G-1 of
+// N(a), clipped to `end`): select the partners whose edge belongs to `a`,
+// flatten their forward lists across the G lanes and probe every element.
+//   lookup(w) -> slot >= 0 on a hit, -1 on a miss
+//   on_hit(slot, w): credit of the third vertex
+// Returns this lane's hit count (the apex credit).  pcnt is a G-entry shared
+// counter array of this group (zero on entry, zero on exit).
+template <int G, bool PER_VERTEX, typename Grp, class Lookup, class OnHit>
+__device__ __forceinline__ unsigned int
+probe_stride(const Grp &grp, long long s, long long end, int a, int da, int fa,
+             const int *__restrict__ ind, const VInfo *__restrict__ vinfo,
+             const int *__restrict__ find, long long n,
+             unsigned long long *__restrict__ tacc, int *pcnt,
+             unsigned int *status, const Lookup &lookup, const OnHit &on_hit)
+{
+    const int lane = grp.thread_rank();
+    const long long e = s + lane;
+    bool partner = false;
+    int x = 0, fx = 0;
+    long long fbx = 0;
+    if (e < end) {
+        x = ind[e];
+        if ((unsigned long long)(long long)x < (unsigned long long)n) {
+            const VInfo ix = vinfo[x];
+            fx = ix.fdeg;
+            fbx = ix.fbeg;
+            const bool fwd = rank_above(ix.deg, x, da, a);
+            partner = fx > 0 && (fwd ? fx <= fa : fx < fa);
+        } else {
+            atomicOr(status, kErrIndexRange);
+        }
+    }
+    const int work = partner ? fx : 0;
+    const int incl = cg::inclusive_scan(grp, work);
+    const int total = grp.shfl(incl, G - 1);
+    const int excl = incl - work;
+    unsigned int hits = 0;
+    for (int f0 = 0; f0 < total; f0 += G) {
+        const int f = f0 + lane;
+        // co-rank: partner i owns flattened index f iff excl_i <= f < incl_i
+        int i = 0;
+#pragma unroll
+        for (int step = G / 2; step >= 1; step >>= 1) {
+            int v = grp.shfl(incl, i + step - 1);
+            if (v <= f) i += step;
+        }
+        const long long fb_i = grp.shfl(fbx, i);
+        const int ex_i = grp.shfl(excl, i);
+        if (f < total) {
+            const int w = find[fb_i + (f - ex_i)];
+            const int slot = lookup(w);
+            if (slot >= 0) {
+                ++hits;
+                if (PER_VERTEX) {
+                    on_hit(slot, w);
+                    atomicAdd(&pcnt[i], 1);
+                }
+            }
+        }
+    }
+    if (PER_VERTEX && total > 0) {
+        grp.sync();
+        const int c = pcnt[lane];
+        if (partner && c > 0) atomicAdd(&tacc[x], (unsigned long long)c);
+        pcnt[lane] = 0;
+        grp.sync();
+    }
+    return hits;
+}
+
+// Group-per-row kernel: G lanes own one apex row at a time; work items are
+// ranges of `item_len` adjacency entries taken from a dynamic queue (a grid
+// partition of the entry space, so a hub row is spread over many items).
+template <int G, int TBL, bool PER_VERTEX, typename OffT>
+__global__ void __launch_bounds__(kRowThreads)
+count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
+                  long long n, long long nnz, const VInfo *__restrict__ vinfo,
+                  const int *__restrict__ find,
+                  unsigned long long *__restrict__ tacc, Counters *ctr,
+                  unsigned int *status, long long n_items, int item_len,
+                  int small_cap)
+{
+    constexpr int kGroups = kRowThreads / G;
+    __shared__ int s_keys[kGroups][TBL];
+    __shared__ int s_hits[kGroups][PER_VERTEX ? TBL : 1];
+    __shared__ int s_pcnt[kGroups][G];
+    auto block = cg::this_thread_block();
+    auto grp = cg::tiled_partition<G>(block);
+    const int gid = grp.meta_group_rank();
+    const int lane = grp.thread_rank();
+    int *keys = s_keys[gid];
+    int *hits = s_hits[gid];
+    int *pcnt = s_pcnt[gid];
+    pcnt[lane] = 0;
+    unsigned long long tri_local = 0;
+
+    while (true) {
+        long long item = 0;
+        if (lane == 0) item = (long long)atomicAdd(&ctr->row_items, 1ull);
+        item = grp.shfl(item, 0);
+        if (item >= n_items) break;
+        const long long e0 = item * item_len;
+        const long long e1 = (e0 + item_len < nnz) ? e0 + item_len : nnz;
+        long long a = row_of_entry(off, n, e0);
+        while (true) {
+            const long long rb = off[a], re = off[a + 1];
+            const long long s0 = rb > e0 ? rb : e0;
+            const long long s1 = re < e1 ? re : e1;
+            const VInfo ia = vinfo[a];
+            const int fa = ia.fdeg;
+            if (s0 < s1 && fa > 0 && fa <= small_cap) {
+                const int log2t = max(ceil_log2(2 * (long long)fa), 2);
+                const int tsize = 1 << log2t;
+                for (int k = lane; k < tsize; k += G) {
+                    keys[k] = -1;
+                    if (PER_VERTEX) hits[k] = 0;
+                }
+                grp.sync();
+                ApexTable tab{keys, hits, log2t, (unsigned int)(tsize - 1)};
+                for (int k = lane; k < fa; k += G) tab.insert(find[ia.fbeg + k]);
+                grp.sync();
+                auto lookup = [&](int w) { return tab.find(w); };
+                auto on_hit = [&](int slot, int) { atomicAdd(&hits[slot], 1); };
+                unsigned int cnt = 0;
+                for (long long s = s0; s < s1; s += G)
+                    cnt += probe_stride<G, PER_VERTEX>(grp, s, s1, (int)a, ia.deg, fa,
+                                                       ind, vinfo, find, n, tacc,
+                                                       pcnt, status, lookup, on_hit);
+                grp.sync();
+                if (PER_VERTEX) {
+                    for (int k = lane; k < tsize; k += G) {
+                        const int h = hits[k];
+                        if (h) atomicAdd(&tacc[keys[k]], (unsigned long long)h);
+                    }
+                    const unsigned int row = cg::reduce(grp, cnt, cg::plus<unsigned int>());
+                    if (lane == 0 && row) atomicAdd(&tacc[a], (unsigned long long)row);
+                }
+                tri_local += cnt;
+                grp.sync();
+            }
+            if (re >= e1) break;
+            // next row holding entry `re` (skips empty rows)
+            a = ((long long)off[a + 2] > re) ? a + 1 : row_of_entry(off, n, re);
+        }
+    }
+    const unsigned long long tri = cg::reduce(grp, tri_local, cg::plus<unsigned long long>());
+    if (lane == 0 && tri) atomicAdd(&ctr->tri_total, tri);
+}
+
+// Block-per-row kernel for apexes whose forward list exceeds small_cap:
+// the whole block shares one table of up to kBigTableSlots slots; beyond
+// kBigHashMaxFdeg the apex list is searched in global memory instead.
+template <bool PER_VERTEX, typename OffT>
+__global__ void __launch_bounds__(kBigThreads)
+count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
+                 long long n, const VInfo *__restrict__ vinfo,
+                 const int *__restrict__ find,
+                 unsigned long long *__restrict__ tacc, Counters *ctr,
+                 unsigned int *status, const long long *__restrict__ big_pre,
+                 int big_chunk, int big_hash_max)
+{
+    extern __shared__ int smem[];
+    int *keys = smem;
+    int *hits = smem + kBigTableSlots;
+    int *pcnt_all = smem + 2 * kBigTableSlots;      // 32 per warp
+    __shared__ long long s_item;
+    __shared__ unsigned int s_cnt;
+    auto block = cg::this_thread_block();
+    auto warp = cg::tiled_partition<32>(block);
+    const int wid = warp.meta_group_rank();
+    const int nwarps = kBigThreads / 32;
+    int *pcnt = pcnt_all + 32 * wid;
+    pcnt[warp.thread_rank()] = 0;
+    const long long n_items = big_pre[n];
+    unsigned long long tri_local = 0;
+
+    while (true) {
+        if (threadIdx.x == 0) {
+            s_item = (long long)atomicAdd(&ctr->big_items, 1ull);
+            s_cnt = 0;
+        }
+        __syncthreads();
+        const long long item = s_item;
+        if (item >= n_items) break;
+        const long long a = row_of_entry(big_pre, n, item);
+        const long long chunk = item - big_pre[a];
+        const long long rb = (long long)off[a] + chunk * big_chunk;
+        long long re = rb + big_chunk;
+        if (re > (long long)off[a + 1]) re = off[a + 1];
+        const VInfo ia = vinfo[a];
+        const int fa = ia.fdeg;
+        unsigned int cnt = 0;
+        if (fa <= big_hash_max) {
+            const int log2t = max(ceil_log2(2 * (long long)fa), 5);
+            const int tsize = 1 << log2t;
+            for (int k = threadIdx.x; k < tsize; k += kBigThreads) {
+                keys[k] = -1;
+                if (PER_VERTEX) hits[k] = 0;
+            }
+            __syncthreads();
+            ApexTable tab{keys, hits, log2t, (unsigned int)(tsize - 1)};
+            for (int k = threadIdx.x; k < fa; k += kBigThreads) tab.insert(find[ia.fbeg + k]);
+            __syncthreads();
+            auto lookup = [&](int w) { return tab.find(w); };
+            auto on_hit = [&](int slot, int) { atomicAdd(&hits[slot], 1); };
+            for (long long s = rb + 32 * wid; s < re; s += 32 * nwarps)
+                cnt += probe_stride<32, PER_VERTEX>(warp, s, re, (int)a, ia.deg, fa, ind,
+                                                    vinfo, find, n, tacc, pcnt, status,
+                                                    lookup, on_hit);
+            __syncthreads();
+            if (PER_VERTEX) {
+                for (int k = threadIdx.x; k < tsize; k += kBigThreads) {
+                    const int h = hits[k];
+                    if (h) atomicAdd(&tacc[keys[k]], (unsigned long long)h);
+                }
+            }
+        } else {
+            const int *list = find + ia.fbeg;
+            auto lookup = [&](int w) { return sorted_find(list, fa, w); };
+            auto on_hit = [&](int, int w) { atomicAdd(&tacc[w], 1ull); };
+            for (long long s = rb + 32 * wid; s < re; s += 32 * nwarps)
+                cnt += probe_stride<32, PER_VERTEX>(warp, s, re, (int)a, ia.deg, fa, ind,
+                                                    vinfo, find, n, tacc, pcnt, status,
+                                                    lookup, on_hit);
+        }
+        const unsigned int wsum = cg::reduce(warp, cnt, cg::plus<unsigned int>());
+        if (warp.thread_rank() == 0 && wsum) atomicAdd(&s_cnt, wsum);
+        __syncthreads();
+        if (threadIdx.x == 0 && s_cnt) {
+            if (PER_VERTEX) atomicAdd(&tacc[a], (unsigned long long)s_cnt);
+            tri_local += s_cnt;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && tri_local) atomicAdd(&ctr->tri_total, tri_local);
+}
+
+// ================================================================ epilogue
+
+__global__ void finalize_kernel(long long n,
+                                const unsigned long long *__restrict__ tacc,
+                                const int *__restrict__ deg,
+                                long long *__restrict__ r,
+                                long long *__restrict__ t,
+                                double *__restrict__ lcc)
+{
+    long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const long long tv = (long long)tacc[v];
+    if (r) r[v] = 2 * tv;
+    if (t) t[v] = tv;
+    if (lcc) {
+        const long long d = deg[v];
+        // one IEEE division of exactly converted integers (bit-identical
+        // to the host formula)
+        lcc[v] = (d < 2) ? 0.0 : __ddiv_rn((double)(2 * tv), (double)(d * (d - 1)));
+    }
+}
+
+__global__ void global_kernel(const Counters *ctr, long long *global)
+{
+    const long long T = (long long)ctr->tri_total;
+    global[0] = T;
+    global[1] = 3 * T;
+    global[2] = 6 * T;
+}
+
+// ================================================================== host
+
+namespace {
+
+int g_sm_count[64];
+int g_rows_blocks[64][8];
+int g_big_blocks[64][2];
+
+int device_sm_count(int dev)
+{
+    if (dev < 0 || dev >= 64) return 148;
+    if (!g_sm_count[dev]) {
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        g_sm_count[dev] = v > 0 ? v : 148;
+    }
+    return g_sm_count[dev];
+}
+
+template <typename K>
+int occupancy_blocks(K kernel, int threads, size_t dyn_smem, int dev, int *cache)
+{
+    if (dev >= 0 && dev < 64 && *cache) return *cache;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, dyn_smem);
+    if (per_sm < 1) per_sm = 1;
+    int blocks = per_sm * device_sm_count(dev);
+    if (dev >= 0 && dev < 64) *cache = blocks;
+    return blocks;
+}
+
+inline size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+}  // namespace
+
+Plan make_plan(long long n, long long nnz, int off_bits, bool per_vertex)
+{
+    Plan p;
+    p.n = n;
+    p.nnz = nnz;
+    p.off_bits = off_bits;
+    p.n_tiles = div_up<long long>(n + nnz, kPrepTile);
+    p.fwd_cap = nnz;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { size_t at = o; o = align256(o + bytes); return at; };
+    p.o_status = take(sizeof(unsigned int));
+    p.o_counters = take(sizeof(Counters));
+    p.o_deg = take(sizeof(int) * (size_t)n);
+    p.o_tile = take(sizeof(long long) * (size_t)(p.n_tiles + 1));
+    long long scan_n = p.n_tiles > n ? p.n_tiles : n;
+    p.o_scan_tmp = take(scan_tmp_bytes(scan_n));
+    p.o_foff = take(sizeof(long long) * (size_t)(n + 1));
+    p.o_vinfo = take(sizeof(VInfo) * (size_t)n);
+    p.o_find = take(sizeof(int) * (size_t)(p.fwd_cap + 4));
+    p.o_tacc = take(per_vertex ? sizeof(unsigned long long) * (size_t)n : 0);
+    p.o_big = take(sizeof(long long) * (size_t)(n + 1));
+    p.bytes = o;
+    return p;
+}
+
+RowConfig pick_row_config(long long n, long long nnz)
+{
+    RowConfig c;
+    const double avg = n > 0 ? (double)nnz / (double)n : 0.0;
+    if (avg <= 24.0) { c.group = 8; c.item_len = 256; }
+    else { c.group = 32; c.item_len = 512; }
+    c.big_chunk = 2048;
+    return c;
+}
+
+template <typename OffT>
+gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz,
+                     bool per_vertex, long long *r, long long *t, double *lcc,
+                     long long *global, void *ws, size_t ws_bytes,
+                     cudaStream_t stream, const RowConfig &cfg, CountTimings *timing)
+{
+    const int off_bits = sizeof(OffT) * 8;
+    Plan p = make_plan(n, nnz, off_bits, per_vertex);
+    if (ws_bytes < p.bytes) return GTC_ERR_WORKSPACE_TOO_SMALL;
+    char *base = static_cast<char *>(ws);
+    unsigned int *status = reinterpret_cast<unsigned int *>(base + p.o_status);
+    Counters *ctr = reinterpret_cast<Counters *>(base + p.o_counters);
+    int *deg = reinterpret_cast<int *>(base + p.o_deg);
+    long long *tile = reinterpret_cast<long long *>(base + p.o_tile);
+    void *scan_tmp = base + p.o_scan_tmp;
+    long long *foff = reinterpret_cast<long long *>(base + p.o_foff);
+    VInfo *vinfo = reinterpret_cast<VInfo *>(base + p.o_vinfo);
+    int *find = reinterpret_cast<int *>(base + p.o_find);
+    unsigned long long *tacc = reinterpret_cast<unsigned long long *>(base + p.o_tacc);
+    long long *big = reinterpret_cast<long long *>(base + p.o_big);
+
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaError_t err;
+    // status word and counters are adjacent at the start of the workspace
+    err = cudaMemsetAsync(base, 0, p.o_deg, stream);
+    if (err != cudaSuccess) return GTC_ERR_CUDA;
+    if (per_vertex && n > 0) {
+        err = cudaMemsetAsync(tacc, 0, sizeof(unsigned long long) * (size_t)n, stream);
+        if (err != cudaSuccess) return GTC_ERR_CUDA;
+    }
+    if (n > 0) {
+        const unsigned vb = (unsigned)div_up<long long>(n, 256);
+        if (timing) cudaEventRecord(timing->ev[0], stream);
+        degree_kernel<<<vb, 256, 0, stream>>>(off, off_bits, n, deg);
+        tile_count_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
+            off, ind, deg, n, nnz, tile, status);
+        err = exclusive_scan_i64(tile, tile, p.n_tiles, scan_tmp, stream);
+        if (err != cudaSuccess) return GTC_ERR_CUDA;
+        tile_fill_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
+            off, ind, deg, n, nnz, tile, foff, find, status);
+        const int small_cap = cfg.group == 32 ? 128 : cfg.group == 16 ? 64 : cfg.group == 8 ? 32 : 16;
+        vinfo_kernel<<<vb, 256, 0, stream>>>(foff, deg, n, small_cap, cfg.big_chunk, vinfo, big);
+        err = exclusive_scan_i64(big, big, n, scan_tmp, stream);
+        if (err != cudaSuccess) return GTC_ERR_CUDA;
+        if (timing) cudaEventRecord(timing->ev[1], stream);
+        if (nnz > 0) {
+            const long long n_items = div_up<long long>(nnz, cfg.item_len);
+            const int slot = (cfg.group == 32 ? 0 : cfg.group == 16 ? 1 : cfg.group == 8 ? 2 : 3) * 2 + (per_vertex ? 1 : 0);
+            auto launch_rows = [&](auto kern) {
+                int blocks = occupancy_blocks(kern, kRowThreads, 0, dev, &g_rows_blocks[dev & 63][slot]);
+                long long need = div_up<long long>(n_items, kRowThreads / cfg.group);
+                if (need < blocks) blocks = (int)need;
+                kern<<<blocks, kRowThreads, 0, stream>>>(off, ind, n, nnz, vinfo, find, tacc, ctr,
+                                                         status, n_items, cfg.item_len, small_cap);
+            };
+#define GTC_ROWS(G, TBL)                                                          \
+    do {                                                                          \
+        if (per_vertex) launch_rows(count_rows_kernel<G, TBL, true, OffT>);       \
+        else launch_rows(count_rows_kernel<G, TBL, false, OffT>);                 \
+    } while (0)
+            switch (cfg.group) {
+            case 32: GTC_ROWS(32, 256); break;
+            case 16: GTC_ROWS(16, 128); break;
+            case 8: GTC_ROWS(8, 64); break;
+            default: GTC_ROWS(4, 32); break;
+            }
+#undef GTC_ROWS
+            if (timing) cudaEventRecord(timing->ev[2], stream);
+            const size_t big_smem = sizeof(int) * (2 * kBigTableSlots + kBigThreads);
+            auto launch_big = [&](auto kern) {
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem);
+                int blocks = occupancy_blocks(kern, kBigThreads, big_smem, dev,
+                                              &g_big_blocks[dev & 63][per_vertex ? 1 : 0]);
+                kern<<<blocks, kBigThreads, big_smem, stream>>>(off, ind, n, vinfo, find, tacc, ctr,
+                                                                status, big, cfg.big_chunk,
+                                                                cfg.big_hash_max);
+            };
+            if (per_vertex) launch_big(count_big_kernel<true, OffT>);
+            else launch_big(count_big_kernel<false, OffT>);
+        } else if (timing) {
+            cudaEventRecord(timing->ev[2], stream);
+        }
+        if (timing) cudaEventRecord(timing->ev[3], stream);
+        if (per_vertex && (r || t || lcc))
+            finalize_kernel<<<vb, 256, 0, stream>>>(n, tacc, deg, r, t, lcc);
+    }
+    if (global) global_kernel<<<1, 1, 0, stream>>>(ctr, global);
+    if (timing) cudaEventRecord(timing->ev[4], stream);
+    err = cudaGetLastError();
+    return err == cudaSuccess ? GTC_OK : GTC_ERR_CUDA;
+}
+
+template gtc_status run_count<int>(const int *, const int *, long long, long long, bool,
+                                   long long *, long long *, double *, long long *, void *,
+                                   size_t, cudaStream_t, const RowConfig &, CountTimings *);
+template gtc_status run_count<long long>(const long long *, const int *, long long, long long,
+                                         bool, long long *, long long *, double *, long long *,
+                                         void *, size_t, cudaStream_t, const RowConfig &,
+                                         CountTimings *);
+
+}  // namespace gtc

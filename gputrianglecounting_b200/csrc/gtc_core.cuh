@@ -1,0 +1,34 @@
+// gtc_core.cuh -- host interface of the single-graph counting pipeline.
+#pragma once
+
+#include "gtc_internal.cuh"
+
+namespace gtc {
+
+// Launch shape of the group-per-row kernel (chosen per graph by the host,
+// overridable by the autotuner).
+struct RowConfig {
+    int group = 32;       // lanes per apex row: 4, 8, 16 or 32
+    int item_len = 512;   // adjacency entries per dynamic work item
+    int big_chunk = 2048; // adjacency entries per block-kernel item
+    int big_hash_max = kBigHashMaxFdeg;  // longest list hashed by the block kernel
+};
+
+// Optional CUDA events recorded between the pipeline phases:
+// ev[0] start, ev[1] forward lists built, ev[2] group kernel done,
+// ev[3] block kernel done, ev[4] epilogue done.
+struct CountTimings {
+    cudaEvent_t ev[5];
+};
+
+Plan make_plan(long long n, long long nnz, int off_bits, bool per_vertex);
+RowConfig pick_row_config(long long n, long long nnz);
+
+template <typename OffT>
+gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz,
+                     bool per_vertex, long long *r, long long *t, double *lcc,
+                     long long *global, void *ws, size_t ws_bytes,
+                     cudaStream_t stream, const RowConfig &cfg,
+                     CountTimings *timing);
+
+}  // namespace gtc

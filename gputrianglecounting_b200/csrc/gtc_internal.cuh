@@ -1,0 +1,119 @@
+// gtc_internal.cuh -- shared device/host helpers of the B200 triangle counter.
+//
+// Algorithm (same output as the reference's per-vertex kernel,
+// src/clusteringCount.cu:314-359, computed differently):
+//   1. orient every undirected edge from the lower to the higher
+//      (degree, id) rank and build the forward lists N+(v) (a filtered copy
+//      of the sorted adjacency, so every N+(v) stays sorted);
+//   2. give every oriented edge u->v to its "apex": the endpoint with the
+//      longer forward list (ties to the source u).  The apex's N+ is staged in
+//      a shared-memory hash table and the partner's (shorter) N+ is probed
+//      into it, so each triangle {u,v,w} is found exactly once, at the edge
+//      between its two lowest-ranked vertices, with sum over edges of
+//      min(d+(u), d+(v)) probes in total;
+//   3. credit the triangle to all three vertices: the apex through a register
+//      count, the partner through a per-partner shared counter, the third
+//      vertex w through a per-slot shared hit counter that is flushed to
+//      global memory once per (apex, w).
+// All counting is integer and exact; the result does not depend on the
+// order in which blocks run.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/gtc_b200.h"
+
+namespace gtc {
+
+// ------------------------------------------------------------------ tuning
+constexpr int kPrepThreads = 256;           // merge-path tile kernels
+constexpr int kPrepItemsPerThread = 8;      // (rows + entries) per thread
+constexpr int kPrepTile = kPrepThreads * kPrepItemsPerThread;
+
+constexpr int kRowThreads = 256;            // group-per-row count kernel
+constexpr int kBigThreads = 512;            // block-per-row count kernel
+constexpr int kBigTableSlots = 8192;        // shared hash slots (block kernel)
+constexpr int kBigHashMaxFdeg = kBigTableSlots / 2;   // load factor <= 1/2
+
+constexpr int kScanThreads = 1024;
+
+// Error bits written to the workspace status word by device code.
+enum : unsigned int {
+    kErrIndexRange = 1u,   // a neighbour id outside [0, n) was met
+    kErrForwardOverflow = 2u,
+};
+
+// Per-vertex record built once per count: forward-list start, forward degree
+// and full degree in one 16-byte load.
+struct __align__(16) VInfo {
+    long long fbeg;
+    int fdeg;
+    int deg;
+};
+
+// Degree-order rank comparison: does x rank above y?
+__device__ __forceinline__ bool rank_above(int dx, int x, int dy, int y)
+{
+    return dx > dy || (dx == dy && x > y);
+}
+
+__device__ __forceinline__ unsigned int hash_slot(int key, int log2_slots)
+{
+    return ((unsigned int)key * 0x9E3779B1u) >> (32 - log2_slots);
+}
+
+__host__ __device__ __forceinline__ int ceil_log2(long long v)
+{
+    int l = 0;
+    while ((1ll << l) < v) ++l;
+    return l;
+}
+
+template <typename T>
+__host__ __device__ __forceinline__ T div_up(T a, T b)
+{
+    return (a + b - 1) / b;
+}
+
+// Largest row r in [0, n) with off[r] <= e (e < off[n]): the row holding e.
+template <typename OffT>
+__device__ __forceinline__ long long row_of_entry(const OffT *__restrict__ off,
+                                                  long long n, long long e)
+{
+    long long lo = 0, hi = n;           // invariant: off[lo] <= e < off[hi]
+    while (hi - lo > 1) {
+        long long mid = (lo + hi) >> 1;
+        if ((long long)off[mid] <= e) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// ------------------------------------------------------------ host helpers
+struct Plan {
+    long long n = 0, nnz = 0;
+    int off_bits = 64;
+    long long n_tiles = 0;       // merge-path tiles over rows + entries
+    long long fwd_cap = 0;       // capacity of the forward adjacency
+    // workspace byte offsets
+    size_t o_status = 0, o_counters = 0, o_deg = 0, o_tile = 0, o_scan_tmp = 0,
+           o_foff = 0, o_vinfo = 0, o_find = 0, o_tacc = 0, o_big = 0,
+           o_bigpre = 0;
+    size_t bytes = 0;
+};
+
+// Counters block in the workspace (device, zeroed at the start of a count).
+struct Counters {
+    unsigned long long tri_total;     // triangles found (T)
+    unsigned long long row_items;     // dynamic item queue, group kernel
+    unsigned long long big_items;     // dynamic item queue, block kernel
+    unsigned long long big_rows;      // number of rows for the block kernel
+    unsigned long long pad[4];
+};
+
+size_t scan_tmp_bytes(long long count);
+cudaError_t exclusive_scan_i64(const long long *in, long long *out,
+                               long long count, void *tmp,
+                               cudaStream_t stream);
+
+}  // namespace gtc

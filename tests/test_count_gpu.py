@@ -1,0 +1,220 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and the
+reference's own outputs.  Integer outputs must be bit-exact; the local
+clustering coefficient must be bit-identical to the host formula (tolerance
+0: one correctly rounded division of exactly converted integers)."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from gputrianglecounting_b200 import api, graphs as G
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TUNINGS = [None, {"group": 4}, {"group": 8}, {"group": 16}, {"group": 32},
+           {"group": 8, "item_len": 64, "big_chunk": 128},
+           {"group": 4, "big_hash_max": 8},     # block kernel's in-place search path
+           {"group": 32, "item_len": 32, "big_chunk": 32, "big_hash_max": 16}]
+
+
+def _dev(off, ind, dev, off_dtype=torch.int64):
+    return (torch.as_tensor(np.asarray(off)).to(dev, off_dtype),
+            torch.as_tensor(np.asarray(ind, np.int32)).to(dev))
+
+
+def _check(off, ind, res, r_ref=None):
+    if r_ref is None:
+        r_ref, t_ref, lcc_ref, total = O.per_vertex(off, ind)
+    else:
+        total = int(r_ref.sum())
+        t_ref = r_ref // 2
+        lcc_ref = O.lcc_formula(r_ref, np.diff(off))
+    torch.cuda.synchronize()
+    assert np.array_equal(res.r.cpu().numpy(), r_ref)
+    assert np.array_equal(res.t.cpu().numpy(), t_ref)
+    assert np.array_equal(res.lcc.cpu().numpy().view(np.int64), lcc_ref.view(np.int64))
+    g = res.global_counts.cpu().numpy()
+    assert g[2] == total and g[0] * 6 == total and g[1] * 2 == total
+
+
+def test_golden_reference_cases(cuda, golden_cases):
+    counter = api.TriangleCounter(cuda)
+    for name, (off, ind, trine, total) in golden_cases.items():
+        r_ref = np.add.reduceat(trine, off[:-1]) if trine.size else np.zeros(len(off) - 1, np.int64)
+        r_ref[np.diff(off) == 0] = 0
+        for off_dtype in (torch.int64, torch.int32):
+            d_off, d_ind = _dev(off, ind, cuda, off_dtype)
+            for tun in TUNINGS:
+                res = counter.count(d_off, d_ind, tuning=tun)
+                _check(off, ind, res, r_ref)
+
+
+@pytest.mark.parametrize("make", [
+    lambda: G.erdos_renyi(16384, 16, 1),         # the ER config itself
+    lambda: G.rmat(14, 16, 2),
+    lambda: G.rmat(16, 16, 3),
+    lambda: G.rgg2d(60000, 12, 3),
+    lambda: G.erdos_renyi(3000, 60, 4),
+])
+def test_random_graphs_vs_oracle(cuda, make):
+    g = make().numpy()
+    r_ref, t_ref, lcc_ref, total = O.per_vertex(g.off, g.ind)
+    counter = api.TriangleCounter(cuda)
+    d_off, d_ind = _dev(g.off, g.ind, cuda)
+    for tun in TUNINGS:
+        res = counter.count(d_off, d_ind, tuning=tun)
+        _check(g.off, g.ind, res, r_ref)
+    res = counter.count(d_off, d_ind, mode="oriented")
+    torch.cuda.synchronize()
+    assert res.r is None and res.oriented_sum == O.oriented_sum(g.off, g.ind)
+    assert res.total == total
+
+
+def test_dense_graph_block_kernel_paths(cuda):
+    """K_n exercises the block kernel (forward lists up to n-1) with both the
+    shared table and the in-place search; closed form t = C(n-1, 2)."""
+    n = 1500
+    off = np.arange(n + 1, dtype=np.int64) * (n - 1)
+    ind = np.concatenate([np.delete(np.arange(n, dtype=np.int32), i) for i in range(n)])
+    d_off, d_ind = _dev(off, ind, cuda)
+    counter = api.TriangleCounter(cuda)
+    for tun in (None, {"big_hash_max": 64}, {"group": 4, "big_chunk": 100}):
+        res = counter.count(d_off, d_ind, tuning=tun)
+        torch.cuda.synchronize()
+        assert (res.t.cpu().numpy() == math.comb(n - 1, 2)).all()
+        assert res.triangles == math.comb(n, 3)
+        assert (res.lcc.cpu().numpy() == 1.0).all()
+
+
+def test_edge_cases(cuda):
+    counter = api.TriangleCounter(cuda)
+    for g in (G.from_edge_list(1, []), G.from_edge_list(9, []), G.from_edge_list(4, [(0, 3)]),
+              G.cycle(3), G.star(70), G.wheel(200)):
+        d_off, d_ind = _dev(g.off, g.ind, cuda)
+        _check(g.off, g.ind, counter.count(d_off, d_ind))
+    # n = 0
+    d_off = torch.zeros(1, dtype=torch.int64, device=cuda)
+    d_ind = torch.zeros(0, dtype=torch.int32, device=cuda)
+    res = counter.count(d_off, d_ind)
+    torch.cuda.synchronize()
+    assert res.r.numel() == 0 and res.triangles == 0
+
+
+def test_deterministic_and_stream(cuda):
+    g = G.rmat(13, 16, 8).to(cuda)
+    counter = api.TriangleCounter(cuda)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        a = counter.count(g.off, g.ind, stream=s)
+    s.synchronize()
+    b = counter.count(g.off, g.ind)
+    torch.cuda.synchronize()
+    assert torch.equal(a.r, b.r) and torch.equal(a.lcc, b.lcc)
+
+
+def test_subset(cuda):
+    g = G.rmat(12, 16, 5).numpy()
+    r_ref, _, _, _ = O.per_vertex(g.off, g.ind)
+    rng = np.random.default_rng(0)
+    v = np.concatenate([[0, 1, g.n - 1], rng.integers(0, g.n, 500)]).astype(np.int32)
+    for off_dtype in (torch.int64, torch.int32):
+        d_off, d_ind = _dev(g.off, g.ind, cuda, off_dtype)
+        out = api.count_subset(d_off, d_ind, torch.as_tensor(v).to(cuda))
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), r_ref[v])
+
+
+def test_compat_kernelCall(cuda):
+    """The reference's kernelCall argument list (src/gpurun.cu:31-37)."""
+    g = G.rmat(12, 12, 6).numpy()
+    r_ref, _, _, _ = O.per_vertex(g.off, g.ind)
+    for dt in (torch.int64, torch.int32):
+        d_off = torch.as_tensor(g.off).to(cuda, dt)
+        d_ind = torch.as_tensor(g.ind).to(cuda, dt)
+        out = torch.full((g.n,), -1, dtype=dt, device=cuda)
+        for bs, tpi in ((256, 1), (32, 32), (96, 4), (1024, 2)):
+            out.fill_(-1)
+            api.kernelCall(g.n, bs, g.n, d_off, d_ind, out, tpi, bs // tpi, int(math.log2(tpi)))
+            torch.cuda.synchronize()
+            assert np.array_equal(out.cpu().numpy().astype(np.int64), r_ref)
+        # vertex-list overload
+        v = torch.as_tensor(np.arange(0, g.n, 7)).to(cuda, dt)
+        vout = torch.zeros(v.numel(), dtype=dt, device=cuda)
+        api.kernelCall(4, 128, v.numel(), d_off, d_ind, vout, 1, 128, 0, vertex=v)
+        torch.cuda.synchronize()
+        assert np.array_equal(vout.cpu().numpy().astype(np.int64), r_ref[::7])
+        # unsupported block size: nothing launched, error reported
+        out.fill_(-1)
+        with pytest.raises(api.GTCError):
+            api.kernelCall(g.n, 100, g.n, d_off, d_ind, out, 1, 100, 0)
+        torch.cuda.synchronize()
+        assert (out.cpu().numpy() == -1).all()
+
+
+@pytest.mark.parametrize("defect,reason", [
+    ("ok", 0), ("offsets", 1), ("range", 2), ("selfloop", 3), ("unsorted", 4), ("asym", 5)])
+def test_validate_csr(cuda, defect, reason):
+    g = G.complete(6).numpy()
+    off, ind = g.off.copy(), g.ind.copy()
+    if defect == "offsets":
+        off[3] = off[4] + 1
+    elif defect == "range":
+        ind[2] = 60
+    elif defect == "selfloop":
+        ind[0] = 0
+    elif defect == "unsorted":
+        ind[0], ind[1] = ind[1], ind[0]
+    elif defect == "asym":
+        off = np.array([0, 1, 2, 3], np.int64); ind = np.array([1, 2, 0], np.int32)
+    for off_dtype in (torch.int64, torch.int32):
+        d_off, d_ind = _dev(off, ind, cuda, off_dtype)
+        assert api.validate_csr(d_off, d_ind)[0] == reason
+
+
+@pytest.mark.skipif(not O.ref_gpu_available(), reason="reference GPU kernel not built")
+def test_reference_gpu_kernel_parity(cuda):
+    """Second oracle: the reference's own kernel (tpi = 1) on the same input."""
+    lib = O.ref_gpu_lib()
+    for g in (G.rmat(13, 16, 2), G.erdos_renyi(16384, 16, 1), G.rgg2d(30000, 12, 3)):
+        gd = g.to(cuda)
+        off64 = gd.off.to(torch.int64)
+        pad = 8
+        ind64 = torch.zeros(g.nnz + 2 * pad, dtype=torch.int64, device=cuda)
+        ind64[pad:pad + g.nnz] = gd.ind.to(torch.int64)
+        ref_out = torch.zeros(g.n, dtype=torch.int64, device=cuda)
+        torch.cuda.synchronize()
+        assert lib.ref_gpu_count_i64(1024, 256, g.n, off64.data_ptr(),
+                                     ind64[pad:].data_ptr(), ref_out.data_ptr()) == 0
+        res = api.count_triangles(gd.off, gd.ind)
+        torch.cuda.synchronize()
+        assert torch.equal(res.r, ref_out)
+
+
+@pytest.mark.parametrize("which", ["rmat20", "rgg4m"])
+def test_full_size_properties(cuda, which):
+    """Full-size configs: size-independent properties (the oracle would take
+    minutes): plain and oriented modes agree, sum t = 3T, r even,
+    t <= C(d, 2), lcc in [0, 1], repeat runs identical, and a seeded row
+    sample matches the oracle's per-row count exactly."""
+    g = (G.rmat(20, 16, 2) if which == "rmat20" else G.rgg2d(1 << 22, 12, 3)).to(cuda)
+    counter = api.TriangleCounter(cuda)
+    a = counter.count(g.off, g.ind)
+    b = counter.count(g.off, g.ind, mode="oriented")
+    torch.cuda.synchronize()
+    T = a.triangles
+    assert b.triangles == T
+    assert int(a.t.sum().item()) == 3 * T
+    assert int((a.r % 2).sum().item()) == 0
+    deg = (g.off[1:] - g.off[:-1])
+    assert bool((a.t <= deg * (deg - 1) // 2).all())
+    assert bool(((a.lcc >= 0) & (a.lcc <= 1)).all())
+    c = counter.count(g.off, g.ind)
+    torch.cuda.synchronize()
+    assert torch.equal(a.r, c.r)
+    rng = np.random.default_rng(11)
+    rows = rng.integers(0, g.n, 300).astype(np.int32)
+    h = g.numpy()
+    sub = O.subset(h.off, h.ind, rows)
+    assert np.array_equal(a.r.cpu().numpy()[rows], sub)
