@@ -19,6 +19,10 @@ inline cudaStream_t as_stream(gtc_stream_t s) { return reinterpret_cast<cudaStre
 
 // ================================================================ validator
 
+// The reason word starts at kNoReason (every byte 0x7f) so that atomicMin
+// keeps the smallest failing reason code; it maps back to GTC_CSR_OK.
+constexpr int kNoReason = 0x7f7f7f7f;
+
 // Phase 1: offsets start at 0, end at nnz, never decrease.
 template <typename OffT>
 __global__ void validate_offsets_kernel(const OffT *__restrict__ off, long long n,
@@ -37,7 +41,7 @@ __global__ void validate_rows_kernel(const OffT *__restrict__ off,
                                      const int *__restrict__ ind, long long n,
                                      int *reason)
 {
-    if (*(volatile int *)reason != GTC_CSR_OK) return;
+    if (*(volatile int *)reason != kNoReason) return;
     const int lane = threadIdx.x & 31;
     const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long a = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < n; a += warps) {
@@ -59,7 +63,7 @@ __global__ void validate_symmetry_kernel(const OffT *__restrict__ off,
                                          const int *__restrict__ ind, long long n,
                                          int *reason)
 {
-    if (*(volatile int *)reason != GTC_CSR_OK) return;
+    if (*(volatile int *)reason != kNoReason) return;
     const int lane = threadIdx.x & 31;
     const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long a = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < n; a += warps) {
@@ -83,7 +87,7 @@ gtc_status run_validate(const OffT *off, const int *ind, long long n, long long 
                         void *ws, int32_t *h_reason, cudaStream_t stream)
 {
     int *reason = static_cast<int *>(ws);
-    cudaError_t e = cudaMemsetAsync(reason, 0, sizeof(int), stream);
+    cudaError_t e = cudaMemsetAsync(reason, 0x7f, sizeof(int), stream);
     if (e != cudaSuccess) return GTC_ERR_CUDA;
     const unsigned vb = (unsigned)div_up<long long>(n + 1, 256);
     validate_offsets_kernel<<<vb, 256, 0, stream>>>(off, n, nnz, reason);
@@ -101,7 +105,7 @@ gtc_status run_validate(const OffT *off, const int *ind, long long n, long long 
     if (e != cudaSuccess) return GTC_ERR_CUDA;
     e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return GTC_ERR_CUDA;
-    *h_reason = host;
+    *h_reason = host == kNoReason ? GTC_CSR_OK : host;
     return GTC_OK;
 }
 

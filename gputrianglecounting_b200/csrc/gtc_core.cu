@@ -231,10 +231,14 @@ __global__ void vinfo_kernel(const long long *__restrict__ foff,
 
 // ============================================================ intersection
 
-// Shared-memory open-addressing table of one apex's forward list.
+// Shared-memory open-addressing table of one apex's forward list: int32 keys
+// (-1 = empty), linear probing, and a 16-bit hit counter per slot packed two
+// to a word.  A counter never exceeds the number of partners probed against
+// one table (<= the entries of one work item < 65536), so the low half never
+// carries into the high half.
 struct ApexTable {
     int *keys;
-    int *hits;
+    unsigned int *hits;
     int log2_slots;
     unsigned int mask;
 
@@ -247,17 +251,32 @@ struct ApexTable {
             slot = (slot + 1) & mask;
         }
     }
+    // Slot of key, or -1.  The first probe resolves almost every lookup at
+    // the load factors used (<= 1/4); the loop only runs for collisions.
     __device__ __forceinline__ int find(int key) const
     {
         unsigned int slot = hash_slot(key, log2_slots);
-        while (true) {
-            int k = keys[slot];
-            if (k == key) return (int)slot;
-            if (k == -1) return -1;
-            slot = (slot + 1) & mask;
+        int k = keys[slot];
+        if (k != key && k != -1) {
+            do {
+                slot = (slot + 1) & mask;
+                k = keys[slot];
+            } while (k != key && k != -1);
         }
+        return k == key ? (int)slot : -1;
     }
+    __device__ __forceinline__ void add_hit(int slot) const
+    {
+        atomicAdd(&hits[slot >> 1], 1u << ((slot & 1) << 4));
+    }
+    __device__ __forceinline__ unsigned int hit_pair(int word) const { return hits[word]; }
 };
+
+// Lanes [lo, hi) of a batch as a bit mask (0 <= lo < hi <= 32).
+__device__ __forceinline__ unsigned int lane_range(int lo, int hi)
+{
+    return (unsigned int)(((1ull << hi) - 1ull) & ~((1ull << lo) - 1ull));
+}
 
 // Binary search of a sorted global forward list (block kernel, apexes whose
 // forward list is larger than the shared table).
@@ -274,19 +293,26 @@ __device__ __forceinline__ int sorted_find(const int *__restrict__ list,
 }
 
 // One stride of up to G adjacency entries of apex `a` (entries s..s+G-1 of
-// N(a), clipped to `end`): select the partners whose edge belongs to `a`,
-// flatten their forward lists across the G lanes and probe every element.
+// N(a), clipped to `end`): select the partners whose edge belongs to `a` and
+// probe every element of their forward lists into the apex's lookup.
+//   * a partner with at least G forward neighbours is swept by the whole
+//     group, G coalesced loads at a time, two in flight;
+//   * the shorter lists are concatenated and swept G probes at a time, each
+//     lane finding its partner by a shuffle binary search over the work
+//     prefix (co-rank).
+// Partner credits: a long partner's hits are one warp reduction; a short
+// partner's hits are the popcount of each batch's hit ballot over the lanes
+// that batch gives it.
 //   lookup(w) -> slot >= 0 on a hit, -1 on a miss
 //   on_hit(slot, w): credit of the third vertex
-// Returns this lane's hit count (the apex credit).  pcnt is a G-entry shared
-// counter array of this group (zero on entry, zero on exit).
+// Returns this lane's hit count (the apex credit).
 template <int G, bool PER_VERTEX, typename Grp, class Lookup, class OnHit>
 __device__ __forceinline__ unsigned int
 probe_stride(const Grp &grp, long long s, long long end, int a, int da, int fa,
              const int *__restrict__ ind, const VInfo *__restrict__ vinfo,
              const int *__restrict__ find, long long n,
-             unsigned long long *__restrict__ tacc, int *pcnt,
-             unsigned int *status, const Lookup &lookup, const OnHit &on_hit)
+             unsigned long long *__restrict__ tacc, unsigned int *status,
+             const Lookup &lookup, const OnHit &on_hit)
 {
     const int lane = grp.thread_rank();
     const long long e = s + lane;
@@ -305,47 +331,107 @@ probe_stride(const Grp &grp, long long s, long long end, int a, int da, int fa,
             atomicOr(status, kErrIndexRange);
         }
     }
-    const int work = partner ? fx : 0;
+    unsigned int hits = 0;
+
+    // (1) long partners, one list at a time
+    unsigned int longs = grp.ballot(partner && fx >= G);
+    while (longs) {
+        const int src = __ffs(longs) - 1;
+        longs &= longs - 1;
+        const int *list = find + grp.shfl(fbx, src);
+        const int len = grp.shfl(fx, src);
+        const int px = grp.shfl(x, src);
+        unsigned int hx = 0;
+        int j = lane;
+        for (; j + G < len; j += 2 * G) {
+            const int w0 = list[j];
+            const int w1 = list[j + G];
+            const int s0 = lookup(w0);
+            const int s1 = lookup(w1);
+            if (s0 >= 0) {
+                ++hx;
+                if (PER_VERTEX) on_hit(s0, w0);
+            }
+            if (s1 >= 0) {
+                ++hx;
+                if (PER_VERTEX) on_hit(s1, w1);
+            }
+        }
+        if (j < len) {
+            const int w0 = list[j];
+            const int s0 = lookup(w0);
+            if (s0 >= 0) {
+                ++hx;
+                if (PER_VERTEX) on_hit(s0, w0);
+            }
+        }
+        if (PER_VERTEX) {
+            const unsigned int hs = cg::reduce(grp, hx, cg::plus<unsigned int>());
+            if (lane == 0 && hs) atomicAdd(&tacc[px], (unsigned long long)hs);
+        }
+        hits += hx;
+    }
+
+    // (2) short partners, flattened
+    const int work = (partner && fx < G) ? fx : 0;
     const int incl = cg::inclusive_scan(grp, work);
     const int total = grp.shfl(incl, G - 1);
     const int excl = incl - work;
-    unsigned int hits = 0;
+    unsigned int mine = 0;
     for (int f0 = 0; f0 < total; f0 += G) {
         const int f = f0 + lane;
-        // co-rank: partner i owns flattened index f iff excl_i <= f < incl_i
+        // co-rank: lane i owns flattened index f iff excl_i <= f < incl_i
         int i = 0;
 #pragma unroll
         for (int step = G / 2; step >= 1; step >>= 1) {
-            int v = grp.shfl(incl, i + step - 1);
+            const int v = grp.shfl(incl, i + step - 1);
             if (v <= f) i += step;
         }
         const long long fb_i = grp.shfl(fbx, i);
         const int ex_i = grp.shfl(excl, i);
+        bool hit = false;
         if (f < total) {
             const int w = find[fb_i + (f - ex_i)];
             const int slot = lookup(w);
             if (slot >= 0) {
-                ++hits;
-                if (PER_VERTEX) {
-                    on_hit(slot, w);
-                    atomicAdd(&pcnt[i], 1);
-                }
+                hit = true;
+                if (PER_VERTEX) on_hit(slot, w);
+            }
+        }
+        hits += hit;
+        if (PER_VERTEX) {
+            const unsigned int hm = grp.ballot(hit);
+            if (work > 0) {
+                const int lo = max(excl - f0, 0), hi = min(incl - f0, G);
+                if (lo < hi) mine += __popc(hm & lane_range(lo, hi));
             }
         }
     }
-    if (PER_VERTEX && total > 0) {
-        grp.sync();
-        const int c = pcnt[lane];
-        if (partner && c > 0) atomicAdd(&tacc[x], (unsigned long long)c);
-        pcnt[lane] = 0;
-        grp.sync();
-    }
+    if (PER_VERTEX && mine) atomicAdd(&tacc[x], (unsigned long long)mine);
     return hits;
+}
+
+// Credit every third vertex w hit in this table (once per (apex, w)) and
+// return nothing; threads [t0, t0 + step) cover the table.
+template <typename T>
+__device__ __forceinline__ void flush_hits(const ApexTable &tab, int tsize, int t0, int step,
+                                          unsigned long long *__restrict__ tacc)
+{
+    for (int wd = t0; wd < (tsize >> 1); wd += step) {
+        const unsigned int pair = tab.hit_pair(wd);
+        if (pair) {
+            const unsigned int lo = pair & 0xffffu, hi = pair >> 16;
+            if (lo) atomicAdd(&tacc[tab.keys[2 * wd]], (unsigned long long)lo);
+            if (hi) atomicAdd(&tacc[tab.keys[2 * wd + 1]], (unsigned long long)hi);
+        }
+    }
 }
 
 // Group-per-row kernel: G lanes own one apex row at a time; work items are
 // ranges of `item_len` adjacency entries taken from a dynamic queue (a grid
 // partition of the entry space, so a hub row is spread over many items).
+// Rows with a forward list longer than small_cap (= 4G) are left to the
+// block kernel.  Table load factor <= 1/4.
 template <int G, int TBL, bool PER_VERTEX, typename OffT>
 __global__ void __launch_bounds__(kRowThreads)
 count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
@@ -357,16 +443,13 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
 {
     constexpr int kGroups = kRowThreads / G;
     __shared__ int s_keys[kGroups][TBL];
-    __shared__ int s_hits[kGroups][PER_VERTEX ? TBL : 1];
-    __shared__ int s_pcnt[kGroups][G];
+    __shared__ unsigned int s_hits[kGroups][PER_VERTEX ? TBL / 2 : 1];
     auto block = cg::this_thread_block();
     auto grp = cg::tiled_partition<G>(block);
     const int gid = grp.meta_group_rank();
     const int lane = grp.thread_rank();
     int *keys = s_keys[gid];
-    int *hits = s_hits[gid];
-    int *pcnt = s_pcnt[gid];
-    pcnt[lane] = 0;
+    unsigned int *hitw = s_hits[gid];
     unsigned long long tri_local = 0;
 
     while (true) {
@@ -384,29 +467,25 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
             const VInfo ia = vinfo[a];
             const int fa = ia.fdeg;
             if (s0 < s1 && fa > 0 && fa <= small_cap) {
-                const int log2t = max(ceil_log2(2 * (long long)fa), 2);
+                const int log2t = max(ceil_log2(4 * (long long)fa), 2);
                 const int tsize = 1 << log2t;
-                for (int k = lane; k < tsize; k += G) {
-                    keys[k] = -1;
-                    if (PER_VERTEX) hits[k] = 0;
-                }
+                for (int k = lane; k < tsize; k += G) keys[k] = -1;
+                if (PER_VERTEX)
+                    for (int k = lane; k < (tsize >> 1); k += G) hitw[k] = 0;
                 grp.sync();
-                ApexTable tab{keys, hits, log2t, (unsigned int)(tsize - 1)};
+                const ApexTable tab{keys, hitw, log2t, (unsigned int)(tsize - 1)};
                 for (int k = lane; k < fa; k += G) tab.insert(find[ia.fbeg + k]);
                 grp.sync();
-                auto lookup = [&](int w) { return tab.find(w); };
-                auto on_hit = [&](int slot, int) { atomicAdd(&hits[slot], 1); };
+                auto lookup = [tab](int w) { return tab.find(w); };
+                auto on_hit = [tab](int slot, int) { tab.add_hit(slot); };
                 unsigned int cnt = 0;
                 for (long long s = s0; s < s1; s += G)
-                    cnt += probe_stride<G, PER_VERTEX>(grp, s, s1, (int)a, ia.deg, fa,
-                                                       ind, vinfo, find, n, tacc,
-                                                       pcnt, status, lookup, on_hit);
+                    cnt += probe_stride<G, PER_VERTEX>(grp, s, s1, (int)a, ia.deg, fa, ind,
+                                                       vinfo, find, n, tacc, status, lookup,
+                                                       on_hit);
                 grp.sync();
                 if (PER_VERTEX) {
-                    for (int k = lane; k < tsize; k += G) {
-                        const int h = hits[k];
-                        if (h) atomicAdd(&tacc[keys[k]], (unsigned long long)h);
-                    }
+                    flush_hits<int>(tab, tsize, lane, G, tacc);
                     const unsigned int row = cg::reduce(grp, cnt, cg::plus<unsigned int>());
                     if (lane == 0 && row) atomicAdd(&tacc[a], (unsigned long long)row);
                 }
@@ -422,9 +501,12 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
     if (lane == 0 && tri) atomicAdd(&ctr->tri_total, tri);
 }
 
-// Block-per-row kernel for apexes whose forward list exceeds small_cap:
-// the whole block shares one table of up to kBigTableSlots slots; beyond
-// kBigHashMaxFdeg the apex list is searched in global memory instead.
+// Block-per-row kernel for apexes whose forward list exceeds small_cap: the
+// whole block shares one table of up to kBigTableSlots slots (load factor
+// <= 1/8 up to kBigTableSlots/8 keys, <= 1/4 up to kBigHashMaxFdeg);
+// beyond big_hash_max the apex list is binary-searched in global memory.
+// Within an item the warps take 32-entry strides from a shared counter, so
+// uneven partner work does not idle the block at its barriers.
 template <bool PER_VERTEX, typename OffT>
 __global__ void __launch_bounds__(kBigThreads)
 count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
@@ -436,16 +518,13 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
 {
     extern __shared__ int smem[];
     int *keys = smem;
-    int *hits = smem + kBigTableSlots;
-    int *pcnt_all = smem + 2 * kBigTableSlots;      // 32 per warp
+    unsigned int *hitw = reinterpret_cast<unsigned int *>(smem + kBigTableSlots);
     __shared__ long long s_item;
     __shared__ unsigned int s_cnt;
+    __shared__ int s_next;
     auto block = cg::this_thread_block();
     auto warp = cg::tiled_partition<32>(block);
-    const int wid = warp.meta_group_rank();
-    const int nwarps = kBigThreads / 32;
-    int *pcnt = pcnt_all + 32 * wid;
-    pcnt[warp.thread_rank()] = 0;
+    const int lane = warp.thread_rank();
     const long long n_items = big_pre[n];
     unsigned long long tri_local = 0;
 
@@ -453,6 +532,7 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
         if (threadIdx.x == 0) {
             s_item = (long long)atomicAdd(&ctr->big_items, 1ull);
             s_cnt = 0;
+            s_next = 0;
         }
         __syncthreads();
         const long long item = s_item;
@@ -465,41 +545,40 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
         const VInfo ia = vinfo[a];
         const int fa = ia.fdeg;
         unsigned int cnt = 0;
+        auto next_stride = [&]() {
+            int st = 0;
+            if (lane == 0) st = atomicAdd(&s_next, 1);
+            return rb + 32ll * warp.shfl(st, 0);
+        };
         if (fa <= big_hash_max) {
-            const int log2t = max(ceil_log2(2 * (long long)fa), 5);
+            const int log2t = min(max(ceil_log2(8 * (long long)fa), 6), kBigTableLog2);
             const int tsize = 1 << log2t;
-            for (int k = threadIdx.x; k < tsize; k += kBigThreads) {
-                keys[k] = -1;
-                if (PER_VERTEX) hits[k] = 0;
-            }
+            for (int k = threadIdx.x; k < tsize; k += kBigThreads) keys[k] = -1;
+            if (PER_VERTEX)
+                for (int k = threadIdx.x; k < (tsize >> 1); k += kBigThreads) hitw[k] = 0;
             __syncthreads();
-            ApexTable tab{keys, hits, log2t, (unsigned int)(tsize - 1)};
+            const ApexTable tab{keys, hitw, log2t, (unsigned int)(tsize - 1)};
             for (int k = threadIdx.x; k < fa; k += kBigThreads) tab.insert(find[ia.fbeg + k]);
             __syncthreads();
-            auto lookup = [&](int w) { return tab.find(w); };
-            auto on_hit = [&](int slot, int) { atomicAdd(&hits[slot], 1); };
-            for (long long s = rb + 32 * wid; s < re; s += 32 * nwarps)
+            auto lookup = [tab](int w) { return tab.find(w); };
+            auto on_hit = [tab](int slot, int) { tab.add_hit(slot); };
+            for (long long s = next_stride(); s < re; s = next_stride())
                 cnt += probe_stride<32, PER_VERTEX>(warp, s, re, (int)a, ia.deg, fa, ind,
-                                                    vinfo, find, n, tacc, pcnt, status,
-                                                    lookup, on_hit);
+                                                    vinfo, find, n, tacc, status, lookup,
+                                                    on_hit);
             __syncthreads();
-            if (PER_VERTEX) {
-                for (int k = threadIdx.x; k < tsize; k += kBigThreads) {
-                    const int h = hits[k];
-                    if (h) atomicAdd(&tacc[keys[k]], (unsigned long long)h);
-                }
-            }
+            if (PER_VERTEX) flush_hits<int>(tab, tsize, threadIdx.x, kBigThreads, tacc);
         } else {
             const int *list = find + ia.fbeg;
-            auto lookup = [&](int w) { return sorted_find(list, fa, w); };
-            auto on_hit = [&](int, int w) { atomicAdd(&tacc[w], 1ull); };
-            for (long long s = rb + 32 * wid; s < re; s += 32 * nwarps)
+            auto lookup = [list, fa](int w) { return sorted_find(list, fa, w); };
+            auto on_hit = [tacc](int, int w) { atomicAdd(&tacc[w], 1ull); };
+            for (long long s = next_stride(); s < re; s = next_stride())
                 cnt += probe_stride<32, PER_VERTEX>(warp, s, re, (int)a, ia.deg, fa, ind,
-                                                    vinfo, find, n, tacc, pcnt, status,
-                                                    lookup, on_hit);
+                                                    vinfo, find, n, tacc, status, lookup,
+                                                    on_hit);
         }
         const unsigned int wsum = cg::reduce(warp, cnt, cg::plus<unsigned int>());
-        if (warp.thread_rank() == 0 && wsum) atomicAdd(&s_cnt, wsum);
+        if (lane == 0 && wsum) atomicAdd(&s_cnt, wsum);
         __syncthreads();
         if (threadIdx.x == 0 && s_cnt) {
             if (PER_VERTEX) atomicAdd(&tacc[a], (unsigned long long)s_cnt);
@@ -672,14 +751,15 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
         else launch_rows(count_rows_kernel<G, TBL, false, OffT>);                 \
     } while (0)
             switch (cfg.group) {
-            case 32: GTC_ROWS(32, 256); break;
-            case 16: GTC_ROWS(16, 128); break;
-            case 8: GTC_ROWS(8, 64); break;
-            default: GTC_ROWS(4, 32); break;
+            case 32: GTC_ROWS(32, 512); break;
+            case 16: GTC_ROWS(16, 256); break;
+            case 8: GTC_ROWS(8, 128); break;
+            default: GTC_ROWS(4, 64); break;
             }
 #undef GTC_ROWS
             if (timing) cudaEventRecord(timing->ev[2], stream);
-            const size_t big_smem = sizeof(int) * (2 * kBigTableSlots + kBigThreads);
+            const size_t big_smem = sizeof(int) * kBigTableSlots +
+                                    sizeof(unsigned int) * (kBigTableSlots / 2);
             auto launch_big = [&](auto kern) {
                 cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem);
                 int blocks = occupancy_blocks(kern, kBigThreads, big_smem, dev,

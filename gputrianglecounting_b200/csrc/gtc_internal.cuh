@@ -33,8 +33,9 @@ constexpr int kPrepTile = kPrepThreads * kPrepItemsPerThread;
 
 constexpr int kRowThreads = 256;            // group-per-row count kernel
 constexpr int kBigThreads = 512;            // block-per-row count kernel
-constexpr int kBigTableSlots = 8192;        // shared hash slots (block kernel)
-constexpr int kBigHashMaxFdeg = kBigTableSlots / 2;   // load factor <= 1/2
+constexpr int kBigTableLog2 = 13;
+constexpr int kBigTableSlots = 1 << kBigTableLog2;   // shared hash slots (block kernel)
+constexpr int kBigHashMaxFdeg = kBigTableSlots / 4;   // load factor <= 1/4
 
 constexpr int kScanThreads = 1024;
 

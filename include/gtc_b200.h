@@ -105,7 +105,7 @@ gtc_status gtc_count(const void *d_off, int off_bits, const int32_t *d_ind,
  *   item_len     adjacency entries per group-kernel work item
  *   big_chunk    adjacency entries per block-kernel work item
  *   big_hash_max longest forward list the block kernel hashes in shared
- *                memory (<= 4096); longer lists are binary-searched in place
+ *                memory (<= 2048); longer lists are binary-searched in place
  */
 typedef struct gtc_tuning {
     int group;

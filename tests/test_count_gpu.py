@@ -42,8 +42,8 @@ def _check(off, ind, res, r_ref=None):
 def test_golden_reference_cases(cuda, golden_cases):
     counter = api.TriangleCounter(cuda)
     for name, (off, ind, trine, total) in golden_cases.items():
-        r_ref = np.add.reduceat(trine, off[:-1]) if trine.size else np.zeros(len(off) - 1, np.int64)
-        r_ref[np.diff(off) == 0] = 0
+        csum = np.concatenate([[0], np.cumsum(trine)])
+        r_ref = csum[off[1:]] - csum[off[:-1]]
         for off_dtype in (torch.int64, torch.int32):
             d_off, d_ind = _dev(off, ind, cuda, off_dtype)
             for tun in TUNINGS:
