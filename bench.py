@@ -339,9 +339,9 @@ def run_b200(args, cfg, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
-# degree, tile count, scan x3, tile fill, vinfo, scan x3, group kernel,
-# block kernel, finalize, global
-LAUNCHES_PER_COUNT = 14
+# degree, tile bounds, tile count, scan x3, tile fill, vinfo, scan x3, group
+# kernel, block kernel, finalize, global
+LAUNCHES_PER_COUNT = 15
 
 
 def phase_breakdown(counter, g, flush) -> dict:

@@ -56,23 +56,33 @@ struct TileSmem {
     long long r0, e0, r1, e1;
 };
 
+// Merge-path coordinates of every tile boundary, all tiles at once (one
+// thread per boundary), so the tile kernels start without a dependent search.
+template <typename OffT>
+__global__ void tile_bounds_kernel(const OffT *__restrict__ off, long long n,
+                                   long long nnz, long long n_tiles,
+                                   long long *__restrict__ trow)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > n_tiles) return;
+    long long d = t * kPrepTile;
+    if (d > n + nnz) d = n + nnz;
+    trow[t] = mp_rows(off, n, nnz, d);
+}
+
 template <typename OffT>
 __device__ void tile_stage(TileSmem &s, const OffT *__restrict__ off,
                            const int *__restrict__ ind, long long n,
-                           long long nnz)
+                           long long nnz, const long long *__restrict__ trow)
 {
     long long d0 = (long long)blockIdx.x * kPrepTile;
     long long d1 = d0 + kPrepTile;
     if (d1 > n + nnz) d1 = n + nnz;
+    const long long r0 = trow[blockIdx.x], r1 = trow[blockIdx.x + 1];
+    const long long e0 = d0 - r0, e1 = d1 - r1;
     if (threadIdx.x == 0) {
-        long long r = mp_rows(off, n, nnz, d0);
-        s.r0 = r; s.e0 = d0 - r;
-    } else if (threadIdx.x == 32) {
-        long long r = mp_rows(off, n, nnz, d1);
-        s.r1 = r; s.e1 = d1 - r;
+        s.r0 = r0; s.e0 = e0; s.r1 = r1; s.e1 = e1;
     }
-    __syncthreads();
-    const long long r0 = s.r0, r1 = s.r1, e0 = s.e0, e1 = s.e1;
     // off[r0 .. r1+1], clamped to off[n]
     for (long long k = threadIdx.x; k <= r1 - r0 + 1; k += blockDim.x) {
         long long r = r0 + k;
@@ -122,10 +132,11 @@ template <typename OffT>
 __global__ void __launch_bounds__(kPrepThreads)
 tile_count_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                   const int *__restrict__ deg, long long n, long long nnz,
+                  const long long *__restrict__ trow,
                   long long *__restrict__ tile_cnt, unsigned int *status)
 {
     __shared__ TileSmem s;
-    tile_stage(s, off, ind, n, nnz);
+    tile_stage(s, off, ind, n, nnz, trow);
     long long li, lj;
     tile_thread_start(s, li, lj);
     const long long rows = s.r1 - s.r0, ents = s.e1 - s.e0;
@@ -160,13 +171,14 @@ template <typename OffT>
 __global__ void __launch_bounds__(kPrepThreads)
 tile_fill_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                  const int *__restrict__ deg, long long n, long long nnz,
+                 const long long *__restrict__ trow,
                  const long long *__restrict__ tile_pre,
                  long long *__restrict__ foff, int *__restrict__ find,
                  unsigned int *status)
 {
     __shared__ TileSmem s;
     __shared__ int warp_sum[kPrepThreads / 32];
-    tile_stage(s, off, ind, n, nnz);
+    tile_stage(s, off, ind, n, nnz, trow);
     long long li, lj;
     tile_thread_start(s, li, lj);
     const long long li0 = li, lj0 = lj;
@@ -675,6 +687,7 @@ Plan make_plan(long long n, long long nnz, int off_bits, bool per_vertex)
     p.o_find = take(sizeof(int) * (size_t)(p.fwd_cap + 4));
     p.o_tacc = take(per_vertex ? sizeof(unsigned long long) * (size_t)n : 0);
     p.o_big = take(sizeof(long long) * (size_t)(n + 1));
+    p.o_trow = take(sizeof(long long) * (size_t)(p.n_tiles + 1));
     p.bytes = o;
     return p;
 }
@@ -709,6 +722,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
     int *find = reinterpret_cast<int *>(base + p.o_find);
     unsigned long long *tacc = reinterpret_cast<unsigned long long *>(base + p.o_tacc);
     long long *big = reinterpret_cast<long long *>(base + p.o_big);
+    long long *trow = reinterpret_cast<long long *>(base + p.o_trow);
 
     int dev = 0;
     cudaGetDevice(&dev);
@@ -724,12 +738,14 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
         const unsigned vb = (unsigned)div_up<long long>(n, 256);
         if (timing) cudaEventRecord(timing->ev[0], stream);
         degree_kernel<<<vb, 256, 0, stream>>>(off, off_bits, n, deg);
+        tile_bounds_kernel<OffT><<<(unsigned)div_up<long long>(p.n_tiles + 1, 256), 256, 0,
+                                   stream>>>(off, n, nnz, p.n_tiles, trow);
         tile_count_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
-            off, ind, deg, n, nnz, tile, status);
+            off, ind, deg, n, nnz, trow, tile, status);
         err = exclusive_scan_i64(tile, tile, p.n_tiles, scan_tmp, stream);
         if (err != cudaSuccess) return GTC_ERR_CUDA;
         tile_fill_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
-            off, ind, deg, n, nnz, tile, foff, find, status);
+            off, ind, deg, n, nnz, trow, tile, foff, find, status);
         const int small_cap = cfg.group == 32 ? 128 : cfg.group == 16 ? 64 : cfg.group == 8 ? 32 : 16;
         vinfo_kernel<<<vb, 256, 0, stream>>>(foff, deg, n, small_cap, cfg.big_chunk, vinfo, big);
         err = exclusive_scan_i64(big, big, n, scan_tmp, stream);

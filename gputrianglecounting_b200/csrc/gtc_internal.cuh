@@ -99,7 +99,7 @@ struct Plan {
     // workspace byte offsets
     size_t o_status = 0, o_counters = 0, o_deg = 0, o_tile = 0, o_scan_tmp = 0,
            o_foff = 0, o_vinfo = 0, o_find = 0, o_tacc = 0, o_big = 0,
-           o_bigpre = 0;
+           o_bigpre = 0, o_trow = 0;
     size_t bytes = 0;
 };
 

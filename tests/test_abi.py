@@ -89,3 +89,19 @@ def test_package_fails_loudly_without_library(tmp_path):
             _lib.load(str(tmp_path / "missing.so"))
         finally:
             _lib._lib = saved
+
+
+def test_reference_style_caller_compiles_and_links(tmp_path):
+    """A caller written like the reference's host run path compiles against
+    include/gtc_b200_kernelcall.hpp and links libgtc_b200.so (no GPU call)."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no g++")
+    lib_dir = os.path.dirname(_lib.LIB_PATH)
+    exe = tmp_path / "kernelcall_user"
+    cmd = ["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "kernelcall_user.cpp"),
+           "-L", lib_dir, "-lgtc_b200", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)]
+    subprocess.run(cmd, check=True, capture_output=True)
+    assert subprocess.run([str(exe)], capture_output=True).returncode == 0
