@@ -439,12 +439,69 @@ __device__ __forceinline__ void flush_hits(const ApexTable &tab, int tsize, int 
     }
 }
 
-// Group-per-row kernel: G lanes own one apex row at a time; work items are
-// ranges of `item_len` adjacency entries taken from a dynamic queue (a grid
-// partition of the entry space, so a hub row is spread over many items).
-// Rows with a forward list longer than small_cap (= 4G) are left to the
-// block kernel.  Table load factor <= 1/4.
-template <int G, int TBL, bool PER_VERTEX, typename OffT>
+// Shuffle co-rank: the lane i whose [incl_i - w_i, incl_i) holds f (incl is
+// this lane's inclusive prefix of a per-lane count; lanes with count 0 are
+// never returned for f < total).
+__device__ __forceinline__ int warp_corank(int incl, int f)
+{
+    int i = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+        const int v = __shfl_sync(0xffffffffu, incl, i + step - 1);
+        if (v <= f) i += step;
+    }
+    return i;
+}
+
+__device__ __forceinline__ int warp_incl_scan(int v)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int o = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= d) v += o;
+    }
+    return v;
+}
+
+// Slot of key in a table region [toff, toff + 2^lg), or -1.
+__device__ __forceinline__ int region_find(const int *keys, int toff, int lg, int key)
+{
+    const unsigned int mask = (1u << lg) - 1u;
+    unsigned int s = hash_slot(key, lg);
+    int k = keys[toff + s];
+    if (k != key && k != -1) {
+        do {
+            s = (s + 1) & mask;
+            k = keys[toff + s];
+        } while (k != key && k != -1);
+    }
+    return k == key ? toff + (int)s : -1;
+}
+
+__device__ __forceinline__ void region_insert(int *keys, int toff, int lg, int key)
+{
+    const unsigned int mask = (1u << lg) - 1u;
+    unsigned int s = hash_slot(key, lg);
+    while (atomicCAS(&keys[toff + s], -1, key) != -1) s = (s + 1) & mask;
+}
+
+// Warp-per-item kernel for apexes with short forward lists (0 < d+ <=
+// small_cap).  A work item is a range of `item_len` adjacency entries taken
+// from a dynamic queue; the warp handles all rows of the item together,
+// up to 32 rows at a time, with warp-uniform control flow:
+//   1. one lane per row loads the row's segment and record; each active row
+//      gets its own region (2^ceil(log2(4 d+)) slots, load factor <= 1/4) of
+//      the warp's shared table, placed by a prefix scan (rows that do not fit
+//      wait for the next batch);
+//   2. the rows' forward lists are inserted as one flattened stream;
+//   3. the rows' entries are scanned 32 at a time for partners, and each
+//      chunk's partner lists are probed as one flattened stream into the
+//      owning row's region (shuffle co-rank over the chunk's work prefix);
+//   4. a partner lane popcounts the hit ballot over its probe range and
+//      credits both itself and its apex; the per-slot 16-bit hit counters
+//      credit the third vertices in one flush per region.
+template <bool PER_VERTEX, typename OffT>
 __global__ void __launch_bounds__(kRowThreads)
 count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                   long long n, long long nnz, const VInfo *__restrict__ vinfo,
@@ -453,64 +510,154 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                   unsigned int *status, long long n_items, int item_len,
                   int small_cap)
 {
-    constexpr int kGroups = kRowThreads / G;
-    __shared__ int s_keys[kGroups][TBL];
-    __shared__ unsigned int s_hits[kGroups][PER_VERTEX ? TBL / 2 : 1];
-    auto block = cg::this_thread_block();
-    auto grp = cg::tiled_partition<G>(block);
-    const int gid = grp.meta_group_rank();
-    const int lane = grp.thread_rank();
-    int *keys = s_keys[gid];
-    unsigned int *hitw = s_hits[gid];
+    constexpr int kWarps = kRowThreads / 32;
+    __shared__ int s_keys[kWarps][kRowSlots];
+    __shared__ unsigned int s_hits[kWarps][PER_VERTEX ? kRowSlots / 2 : 1];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int *keys = s_keys[wid];
+    unsigned int *hitw = s_hits[wid];
     unsigned long long tri_local = 0;
 
     while (true) {
         long long item = 0;
         if (lane == 0) item = (long long)atomicAdd(&ctr->row_items, 1ull);
-        item = grp.shfl(item, 0);
+        item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= n_items) break;
         const long long e0 = item * item_len;
         const long long e1 = (e0 + item_len < nnz) ? e0 + item_len : nnz;
-        long long a = row_of_entry(off, n, e0);
+        long long ra = row_of_entry(off, n, e0);
         while (true) {
-            const long long rb = off[a], re = off[a + 1];
+            // ---- 1. rows of this batch (lane = row ra + lane)
+            const long long r = ra + lane;
+            const bool exists = r < n;
+            const long long rb = exists ? (long long)off[r] : nnz;
+            const long long re = exists ? (long long)off[r + 1] : nnz;
+            const bool in_item = exists && rb < e1;
             const long long s0 = rb > e0 ? rb : e0;
             const long long s1 = re < e1 ? re : e1;
-            const VInfo ia = vinfo[a];
-            const int fa = ia.fdeg;
-            if (s0 < s1 && fa > 0 && fa <= small_cap) {
-                const int log2t = max(ceil_log2(4 * (long long)fa), 2);
-                const int tsize = 1 << log2t;
-                for (int k = lane; k < tsize; k += G) keys[k] = -1;
+            const int len = (in_item && s1 > s0) ? (int)(s1 - s0) : 0;
+            VInfo vi{0, 0, 0};
+            if (len > 0) vi = vinfo[r];
+            bool act = len > 0 && vi.fdeg > 0 && vi.fdeg <= small_cap;
+            const int lg = act ? max(ceil_log2(4 * (long long)vi.fdeg), 2) : 0;
+            const int ts = act ? (1 << lg) : 0;
+            const int tincl = warp_incl_scan(ts);
+            const int toff = tincl - ts;
+            const bool take = in_item && tincl <= kRowSlots;
+            const unsigned int tmask = __ballot_sync(0xffffffffu, take);
+            const int nrows = __popc(tmask);          // a prefix of the lanes
+            if (nrows == 0) break;                    // row ra starts at or after e1
+            act = act && take;
+            const int total_slots = (int)__reduce_max_sync(0xffffffffu, act ? (unsigned)tincl : 0u);
+            if (total_slots > 0) {
+                for (int k = lane; k < total_slots; k += 32) keys[k] = -1;
                 if (PER_VERTEX)
-                    for (int k = lane; k < (tsize >> 1); k += G) hitw[k] = 0;
-                grp.sync();
-                const ApexTable tab{keys, hitw, log2t, (unsigned int)(tsize - 1)};
-                for (int k = lane; k < fa; k += G) tab.insert(find[ia.fbeg + k]);
-                grp.sync();
-                auto lookup = [tab](int w) { return tab.find(w); };
-                auto on_hit = [tab](int slot, int) { tab.add_hit(slot); };
-                unsigned int cnt = 0;
-                for (long long s = s0; s < s1; s += G)
-                    cnt += probe_stride<G, PER_VERTEX>(grp, s, s1, (int)a, ia.deg, fa, ind,
-                                                       vinfo, find, n, tacc, status, lookup,
-                                                       on_hit);
-                grp.sync();
-                if (PER_VERTEX) {
-                    flush_hits<int>(tab, tsize, lane, G, tacc);
-                    const unsigned int row = cg::reduce(grp, cnt, cg::plus<unsigned int>());
-                    if (lane == 0 && row) atomicAdd(&tacc[a], (unsigned long long)row);
+                    for (int k = lane; k < (total_slots >> 1); k += 32) hitw[k] = 0;
+                __syncwarp();
+                // ---- 2. insert the forward lists of the active rows
+                const int fw = act ? vi.fdeg : 0;
+                const int fincl = warp_incl_scan(fw);
+                const int ftot = __shfl_sync(0xffffffffu, fincl, 31);
+                const int fexcl = fincl - fw;
+                for (int f0 = 0; f0 < ftot; f0 += 32) {
+                    const int f = f0 + lane;
+                    const int i = warp_corank(fincl, f);
+                    const long long fb_i = __shfl_sync(0xffffffffu, vi.fbeg, i);
+                    const int ex_i = __shfl_sync(0xffffffffu, fexcl, i);
+                    const int to_i = __shfl_sync(0xffffffffu, toff, i);
+                    const int lg_i = __shfl_sync(0xffffffffu, lg, i);
+                    if (f < ftot) region_insert(keys, to_i, lg_i, find[fb_i + (f - ex_i)]);
                 }
-                tri_local += cnt;
-                grp.sync();
+                __syncwarp();
+                // ---- 3. scan the active rows' entries for partners, probe
+                const int lw = act ? len : 0;
+                const int lincl = warp_incl_scan(lw);
+                const int ltot = __shfl_sync(0xffffffffu, lincl, 31);
+                const int lexcl = lincl - lw;
+                for (int c0 = 0; c0 < ltot; c0 += 32) {
+                    const int f = c0 + lane;
+                    const int i = warp_corank(lincl, f);
+                    const long long s0_i = __shfl_sync(0xffffffffu, s0, i);
+                    const int ex_i = __shfl_sync(0xffffffffu, lexcl, i);
+                    const int fa_i = __shfl_sync(0xffffffffu, vi.fdeg, i);
+                    const int da_i = __shfl_sync(0xffffffffu, vi.deg, i);
+                    const int to_i = __shfl_sync(0xffffffffu, toff, i);
+                    const int lg_i = __shfl_sync(0xffffffffu, lg, i);
+                    const int a = (int)(ra + i);
+                    bool partner = false;
+                    int x = 0, fx = 0;
+                    long long fbx = 0;
+                    if (f < ltot) {
+                        x = ind[s0_i + (f - ex_i)];
+                        if ((unsigned long long)(long long)x < (unsigned long long)n) {
+                            const VInfo ix = vinfo[x];
+                            fx = ix.fdeg;
+                            fbx = ix.fbeg;
+                            const bool fwd = rank_above(ix.deg, x, da_i, a);
+                            partner = fx > 0 && (fwd ? fx <= fa_i : fx < fa_i);
+                        } else {
+                            atomicOr(status, kErrIndexRange);
+                        }
+                    }
+                    const int pw = partner ? fx : 0;
+                    const int pincl = warp_incl_scan(pw);
+                    const int ptot = __shfl_sync(0xffffffffu, pincl, 31);
+                    const int pexcl = pincl - pw;
+                    unsigned int mine = 0;
+                    for (int g0 = 0; g0 < ptot; g0 += 32) {
+                        const int g = g0 + lane;
+                        const int p = warp_corank(pincl, g);
+                        const long long fb_p = __shfl_sync(0xffffffffu, fbx, p);
+                        const int ex_p = __shfl_sync(0xffffffffu, pexcl, p);
+                        const int to_p = __shfl_sync(0xffffffffu, to_i, p);
+                        const int lg_p = __shfl_sync(0xffffffffu, lg_i, p);
+                        bool hit = false;
+                        if (g < ptot) {
+                            const int slot = region_find(keys, to_p, lg_p, find[fb_p + (g - ex_p)]);
+                            if (slot >= 0) {
+                                hit = true;
+                                if (PER_VERTEX) atomicAdd(&hitw[slot >> 1], 1u << ((slot & 1) << 4));
+                            }
+                        }
+                        const unsigned int hm = __ballot_sync(0xffffffffu, hit);
+                        if (pw > 0) {
+                            const int lo = max(pexcl - g0, 0), hi = min(pincl - g0, 32);
+                            if (lo < hi) mine += __popc(hm & lane_range(lo, hi));
+                        }
+                    }
+                    if (mine) {
+                        if (PER_VERTEX) {
+                            atomicAdd(&tacc[x], (unsigned long long)mine);
+                            atomicAdd(&tacc[a], (unsigned long long)mine);
+                        }
+                        tri_local += mine;
+                    }
+                }
+                __syncwarp();
+                // ---- 4. third-vertex credits
+                if (PER_VERTEX) {
+                    for (int k = lane; k < (total_slots >> 1); k += 32) {
+                        const unsigned int pair = hitw[k];
+                        if (pair) {
+                            const unsigned int lo = pair & 0xffffu, hi = pair >> 16;
+                            if (lo) atomicAdd(&tacc[keys[2 * k]], (unsigned long long)lo);
+                            if (hi) atomicAdd(&tacc[keys[2 * k + 1]], (unsigned long long)hi);
+                        }
+                    }
+                }
+                __syncwarp();
             }
-            if (re >= e1) break;
-            // next row holding entry `re` (skips empty rows)
-            a = ((long long)off[a + 2] > re) ? a + 1 : row_of_entry(off, n, re);
+            // ---- next batch: the row after the last taken one
+            const long long last = ra + nrows - 1;
+            const long long last_end = __shfl_sync(0xffffffffu, re, nrows - 1);
+            if (last_end >= e1 || last + 1 >= n) break;
+            ra = last + 1;
+            if ((long long)off[ra + 1] == last_end) ra = row_of_entry(off, n, last_end);
         }
     }
-    const unsigned long long tri = cg::reduce(grp, tri_local, cg::plus<unsigned long long>());
-    if (lane == 0 && tri) atomicAdd(&ctr->tri_total, tri);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) tri_local += __shfl_down_sync(0xffffffffu, tri_local, d);
+    if (lane == 0 && tri_local) atomicAdd(&ctr->tri_total, tri_local);
 }
 
 // Block-per-row kernel for apexes whose forward list exceeds small_cap: the
@@ -746,33 +893,23 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
         if (err != cudaSuccess) return GTC_ERR_CUDA;
         tile_fill_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
             off, ind, deg, n, nnz, trow, tile, foff, find, status);
-        const int small_cap = cfg.group == 32 ? 128 : cfg.group == 16 ? 64 : cfg.group == 8 ? 32 : 16;
+        const int small_cap = 4 * cfg.group;   // <= kRowSlots / 8
         vinfo_kernel<<<vb, 256, 0, stream>>>(foff, deg, n, small_cap, cfg.big_chunk, vinfo, big);
         err = exclusive_scan_i64(big, big, n, scan_tmp, stream);
         if (err != cudaSuccess) return GTC_ERR_CUDA;
         if (timing) cudaEventRecord(timing->ev[1], stream);
         if (nnz > 0) {
             const long long n_items = div_up<long long>(nnz, cfg.item_len);
-            const int slot = (cfg.group == 32 ? 0 : cfg.group == 16 ? 1 : cfg.group == 8 ? 2 : 3) * 2 + (per_vertex ? 1 : 0);
             auto launch_rows = [&](auto kern) {
-                int blocks = occupancy_blocks(kern, kRowThreads, 0, dev, &g_rows_blocks[dev & 63][slot]);
-                long long need = div_up<long long>(n_items, kRowThreads / cfg.group);
+                int blocks = occupancy_blocks(kern, kRowThreads, 0, dev,
+                                              &g_rows_blocks[dev & 63][per_vertex ? 1 : 0]);
+                long long need = div_up<long long>(n_items, kRowThreads / 32);
                 if (need < blocks) blocks = (int)need;
                 kern<<<blocks, kRowThreads, 0, stream>>>(off, ind, n, nnz, vinfo, find, tacc, ctr,
                                                          status, n_items, cfg.item_len, small_cap);
             };
-#define GTC_ROWS(G, TBL)                                                          \
-    do {                                                                          \
-        if (per_vertex) launch_rows(count_rows_kernel<G, TBL, true, OffT>);       \
-        else launch_rows(count_rows_kernel<G, TBL, false, OffT>);                 \
-    } while (0)
-            switch (cfg.group) {
-            case 32: GTC_ROWS(32, 512); break;
-            case 16: GTC_ROWS(16, 256); break;
-            case 8: GTC_ROWS(8, 128); break;
-            default: GTC_ROWS(4, 64); break;
-            }
-#undef GTC_ROWS
+            if (per_vertex) launch_rows(count_rows_kernel<true, OffT>);
+            else launch_rows(count_rows_kernel<false, OffT>);
             if (timing) cudaEventRecord(timing->ev[2], stream);
             const size_t big_smem = sizeof(int) * kBigTableSlots +
                                     sizeof(unsigned int) * (kBigTableSlots / 2);

@@ -31,7 +31,8 @@ constexpr int kPrepThreads = 256;           // merge-path tile kernels
 constexpr int kPrepItemsPerThread = 8;      // (rows + entries) per thread
 constexpr int kPrepTile = kPrepThreads * kPrepItemsPerThread;
 
-constexpr int kRowThreads = 256;            // group-per-row count kernel
+constexpr int kRowThreads = 256;            // warp-per-item count kernel
+constexpr int kRowSlots = 1024;             // shared table slots per warp
 constexpr int kBigThreads = 512;            // block-per-row count kernel
 constexpr int kBigTableLog2 = 13;
 constexpr int kBigTableSlots = 1 << kBigTableLog2;   // shared hash slots (block kernel)
