@@ -34,6 +34,7 @@ _SIGNATURES = {
     "gtc_count_tuned": (c_int, [P, c_int, P, c_int64, c_int64, c_int, P, P, P, P, P, c_size_t, P,
                                 P]),
     "gtc_count_phase_times": (c_int, [P, c_int, P, c_int64, c_int64, P, c_size_t, P]),
+    "gtc_count_noalloc": (c_int, [P, c_int, P, c_int64, c_int64, c_int, P, P, P, P, P]),
     "gtc_count_subset": (c_int, [P, c_int, P, P, c_int64, P, P]),
     "gtc_validate_workspace_size": (c_size_t, [c_int64, c_int64]),
     "gtc_validate_csr": (c_int, [P, c_int, P, c_int64, c_int64, P, c_size_t, P, P]),

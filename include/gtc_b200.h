@@ -134,6 +134,25 @@ gtc_status gtc_count_phase_times(const void *d_off, int off_bits,
                                  float *h_ms);
 
 /*
+ * gtc_count with no device allocation at all, for callers that cannot
+ * allocate when they count (a serving loop that reserved its memory at start-up,
+ * a plug-in whose host framework owns the device memory, or a caller that must
+ * avoid the synchronisation cudaMalloc/cudaFree can cause).  This entry point
+ * has no counterpart in the reference.  The pipeline's scratch lives in a
+ * fixed 32 MiB array inside the library: graphs whose gtc_workspace_size
+ * exceeds it are rejected with GTC_ERR_CAPACITY.  Every device that loads the
+ * library holds the array until exit.  All calls on a device share it, so
+ * calls that overlap on the GPU race and must be serialised.  The first call
+ * on each device looks up the array's address; make it before any stream
+ * capture.  Arguments and outputs as gtc_count; asynchronous on `stream`.
+ */
+gtc_status gtc_count_noalloc(const void *d_off, int off_bits,
+                             const int32_t *d_ind, int64_t n, int64_t nnz,
+                             gtc_mode mode, int64_t *d_r, int64_t *d_t,
+                             double *d_lcc, int64_t *d_global,
+                             gtc_stream_t stream);
+
+/*
  * Per-vertex counts for a vertex subset: d_out[k] = r(d_vertex[k]) for
  * k < count.  Replaces the vertex-list kernelCall overload
  * (src/clusteringCount.cu:361-413, kernel :266-312).  Like the reference it
