@@ -35,6 +35,11 @@ _SIGNATURES = {
                                 P]),
     "gtc_count_phase_times": (c_int, [P, c_int, P, c_int64, c_int64, P, c_size_t, P]),
     "gtc_count_noalloc": (c_int, [P, c_int, P, c_int64, c_int64, c_int, P, P, P, P, P]),
+    "gtc_batch_workspace_size": (c_int, [c_int64, c_int64, c_int64, P]),
+    "gtc_count_batch": (c_int, [c_int64, P, P, P, c_int64, c_int64, P, P, P, P, P, c_size_t, P,
+                                P]),
+    "gtc_batch_pack_scratch_bytes": (c_size_t, [c_int64]),
+    "gtc_batch_pack": (c_int, [c_int64, P, P, P, P, P, P, P, P, c_size_t, P, P]),
     "gtc_count_subset": (c_int, [P, c_int, P, P, c_int64, P, P]),
     "gtc_validate_workspace_size": (c_size_t, [c_int64, c_int64]),
     "gtc_validate_csr": (c_int, [P, c_int, P, c_int64, c_int64, P, c_size_t, P, P]),

@@ -206,3 +206,120 @@ def kernelCall(numberBlocks: int, numberThreads: int, nv: int, d_off: torch.Tens
            d_ind.data_ptr(), outPutTriangles.data_ptr(), threads_per_block, number_blocks,
            shifter)
     check(lib.gtc_compat_last_status(), "kernelCall")
+
+
+# ------------------------------------------------------------------ batched
+
+@dataclass
+class BatchCSR:
+    """Many graphs in one concatenated CSR (device tensors).
+
+    vstart[G+1] int64 vertex starts, off[N+1] int64 offsets into the
+    concatenated adjacency, ind[NNZ] int32 graph-local neighbour ids.
+    """
+
+    vstart: torch.Tensor
+    off: torch.Tensor
+    ind: torch.Tensor
+
+    @property
+    def num_graphs(self) -> int:
+        return int(self.vstart.numel()) - 1
+
+    @property
+    def total_n(self) -> int:
+        return int(self.off.numel()) - 1
+
+    @property
+    def total_nnz(self) -> int:
+        return int(self.ind.numel())
+
+    def graph(self, g: int):
+        """Graph g alone as a CSRGraph (offsets rebased to 0, same device)."""
+        from .graphs import CSRGraph
+        v0, v1 = int(self.vstart[g]), int(self.vstart[g + 1])
+        off = self.off[v0:v1 + 1]
+        e0, e1 = int(off[0]), int(off[-1])
+        return CSRGraph((off - e0).contiguous(), self.ind[e0:e1].contiguous(), f"g{g}")
+
+
+@dataclass
+class BatchCounts:
+    r: torch.Tensor | None          # int64[N] over the concatenated vertex space
+    t: torch.Tensor | None
+    lcc: torch.Tensor | None
+    graph_T: torch.Tensor | None    # int64[G]
+
+
+class BatchCounter:
+    """Counts a whole batch of graphs in one pipeline run (one device)."""
+
+    def __init__(self, device=None):
+        _lib.load()
+        self.device = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+        self._ws: torch.Tensor | None = None
+        self._pack_scratch: torch.Tensor | None = None
+        self._pack_staging: torch.Tensor | None = None
+
+    def workspace_bytes(self, num_graphs: int, total_n: int, total_nnz: int) -> int:
+        out = ctypes.c_size_t(0)
+        check(_lib.load().gtc_batch_workspace_size(num_graphs, total_n, total_nnz,
+                                                   ctypes.byref(out)), "gtc_batch_workspace_size")
+        return int(out.value)
+
+    def reserve(self, num_graphs: int, total_n: int, total_nnz: int) -> None:
+        """Allocate the workspace up front (e.g. before a CUDA-graph capture)."""
+        need = self.workspace_bytes(num_graphs, total_n, total_nnz)
+        if self._ws is None or self._ws.numel() < need:
+            self._ws = None
+            self._ws = torch.empty(max(need, 256), dtype=torch.uint8, device=self.device)
+
+    def alloc_outputs(self, batch: BatchCSR, outputs=("r", "lcc", "graph_T")) -> BatchCounts:
+        dev, n, G = self.device, batch.total_n, batch.num_graphs
+        return BatchCounts(
+            r=torch.empty(n, dtype=torch.int64, device=dev) if "r" in outputs else None,
+            t=torch.empty(n, dtype=torch.int64, device=dev) if "t" in outputs else None,
+            lcc=torch.empty(n, dtype=torch.float64, device=dev) if "lcc" in outputs else None,
+            graph_T=torch.empty(G, dtype=torch.int64, device=dev) if "graph_T" in outputs else None)
+
+    def count(self, batch: BatchCSR, outputs=("r", "lcc", "graph_T"), out: BatchCounts | None = None,
+              tuning: dict | None = None, stream=None) -> BatchCounts:
+        G, n, nnz = batch.num_graphs, batch.total_n, batch.total_nnz
+        self.reserve(G, n, nnz)
+        if out is None:
+            out = self.alloc_outputs(batch, outputs)
+        tun = _lib.Tuning(**{k: int(v) for k, v in tuning.items()}) if tuning else None
+        check(_lib.load().gtc_count_batch(
+            G, batch.vstart.data_ptr(), batch.off.data_ptr(),
+            batch.ind.data_ptr() if nnz else None, n, nnz, _ptr(out.r), _ptr(out.t),
+            _ptr(out.lcc), _ptr(out.graph_T), self._ws.data_ptr(), self._ws.numel(),
+            ctypes.byref(tun) if tun is not None else None, _stream_handle(stream)),
+            "gtc_count_batch")
+        return out
+
+    def pack(self, graphs, stream=None) -> BatchCSR:
+        """Concatenate separate device-resident graphs (int64 off, int32 ind)."""
+        G = len(graphs)
+        lib = _lib.load()
+        need = int(lib.gtc_batch_pack_scratch_bytes(G))
+        if self._pack_scratch is None or self._pack_scratch.numel() < need:
+            self._pack_scratch = torch.empty(need, dtype=torch.uint8, device=self.device)
+            self._pack_staging = torch.empty(need, dtype=torch.uint8).pin_memory()
+        else:
+            # the staging buffer may still feed an earlier copy
+            torch.cuda.current_stream(self.device).synchronize()
+        offs = (ctypes.c_void_p * max(G, 1))(*[g.off.data_ptr() for g in graphs])
+        inds = (ctypes.c_void_p * max(G, 1))(*[g.ind.data_ptr() for g in graphs])
+        ns = (ctypes.c_int64 * max(G, 1))(*[g.n for g in graphs])
+        nnzs = (ctypes.c_int64 * max(G, 1))(*[g.nnz for g in graphs])
+        total_n, total_nnz = sum(g.n for g in graphs), sum(g.nnz for g in graphs)
+        vstart = torch.empty(G + 1, dtype=torch.int64, device=self.device)
+        off = torch.empty(total_n + 1, dtype=torch.int64, device=self.device)
+        ind = torch.empty(max(total_nnz, 1), dtype=torch.int32, device=self.device)[:total_nnz]
+        check(lib.gtc_batch_pack(G, offs, inds, ns, nnzs, vstart.data_ptr(), off.data_ptr(),
+                                 ind.data_ptr() if total_nnz else None,
+                                 self._pack_scratch.data_ptr(), self._pack_scratch.numel(),
+                                 self._pack_staging.data_ptr(), _stream_handle(stream)),
+              "gtc_batch_pack")
+        return BatchCSR(vstart, off, ind)

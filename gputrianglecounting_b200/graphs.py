@@ -319,3 +319,65 @@ def forward_stats(gph: CSRGraph) -> dict:
         "W_fwd_merge": int((dplus[fr] + dplus[fc]).sum()),
         "probe_vtx_centric": int(dplus[fc].sum()),
     }
+
+
+# ------------------------------------------------------------------ batches
+
+def batched_specs(num_graphs: int = 4096, seed: int = 4, n_lo: int = 256,
+                  n_hi: int = 262_144) -> list[dict]:
+    """Parameters of the batched workload: vertex counts log-uniform in
+    [n_lo, n_hi]; half the graphs Erdos-Renyi with mean degree uniform in
+    [8, 32], half R-MAT (0.57, 0.19, 0.19, 0.05) with edge factor uniform in
+    [8, 16]; one derived seed per graph."""
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(math.log(n_lo), math.log(n_hi), num_graphs)).astype(np.int64)
+    kinds = np.array(["er"] * (num_graphs // 2) + ["rmat"] * (num_graphs - num_graphs // 2))
+    rng.shuffle(kinds)
+    er_deg = rng.uniform(8.0, 32.0, num_graphs)
+    ef = rng.uniform(8.0, 16.0, num_graphs)
+    specs = []
+    for g in range(num_graphs):
+        s = {"kind": str(kinds[g]), "n": int(max(n[g], 2)), "seed": int(seed) * 1_000_003 + g}
+        if s["kind"] == "er":
+            s["mean_degree"] = float(er_deg[g])
+        else:
+            s["edge_factor"] = float(ef[g])
+        specs.append(s)
+    return specs
+
+
+def make_spec_graph(spec: dict, device="cpu") -> CSRGraph:
+    n = spec["n"]
+    if spec["kind"] == "er":
+        return erdos_renyi(n, min(spec["mean_degree"], n - 1), spec["seed"], device)
+    device = torch.device(device)
+    scale = max(1, int(math.ceil(math.log2(n))))
+    g = _gen(spec["seed"], device)
+    src, dst = rmat_pairs(scale, int(round(spec["edge_factor"] * n)), (0.57, 0.19, 0.19, 0.05),
+                          g, device)
+    keep = (src < n) & (dst < n)
+    return csr_from_pairs(src[keep], dst[keep], n, name=f"rmat_n{n}_s{spec['seed']}")
+
+
+def concat_graphs(graphs: list[CSRGraph], device=None):
+    """(vstart, off, ind) of the concatenated layout with graph-local ids."""
+    from .api import BatchCSR
+    device = torch.device(device) if device is not None else graphs[0].off.device
+    ns = torch.tensor([0] + [g.n for g in graphs], dtype=torch.int64)
+    es = torch.tensor([0] + [g.nnz for g in graphs], dtype=torch.int64)
+    vstart = torch.cumsum(ns, 0).to(device)
+    ebase = torch.cumsum(es, 0)
+    offs = [torch.as_tensor(g.off)[:-1].to(device) + int(ebase[i]) for i, g in enumerate(graphs)]
+    offs.append(torch.tensor([int(ebase[-1])], dtype=torch.int64, device=device))
+    off = torch.cat(offs)
+    ind = torch.cat([torch.as_tensor(g.ind).to(device) for g in graphs]) if graphs else \
+        torch.zeros(0, dtype=torch.int32, device=device)
+    return BatchCSR(vstart, off, ind)
+
+
+def batched(num_graphs: int = 4096, seed: int = 4, device="cpu", n_lo: int = 256,
+            n_hi: int = 262_144):
+    """The batched workload as one BatchCSR (built graph by graph on `device`)."""
+    specs = batched_specs(num_graphs, seed, n_lo, n_hi)
+    graphs = [make_spec_graph(s, device) for s in specs]
+    return concat_graphs(graphs, device), specs

@@ -165,6 +165,44 @@ gtc_status gtc_count_subset(const void *d_off, int off_bits,
                             gtc_stream_t stream);
 
 /*
+ * Batched counting: many independent graphs in one pipeline run (no
+ * counterpart in the reference, whose host path counts one graph per
+ * kernelCall, src/gpurun.cu:2-56).
+ *   d_vstart[G+1]   int64 vertex starts of the graphs in the concatenated
+ *                   vertex space (d_vstart[0] = 0, d_vstart[G] = total_n)
+ *   d_off[total_n+1] int64 offsets into the concatenated adjacency
+ *   d_ind[total_nnz] int32 graph-local neighbour ids (0 .. n_g-1)
+ *   d_r, d_t, d_lcc  per-vertex outputs over the concatenated vertex space
+ *                   (nullable); d_graph_T[G] triangles per graph (nullable)
+ * Every graph obeys the single-graph contract; total_n < 2^31.  The result
+ * for each graph is exactly the one gtc_count gives for it alone.
+ * Asynchronous on `stream`; capturable in a CUDA graph after one warm-up call.
+ */
+gtc_status gtc_batch_workspace_size(int64_t num_graphs, int64_t total_n,
+                                    int64_t total_nnz, size_t *bytes);
+gtc_status gtc_count_batch(int64_t num_graphs, const int64_t *d_vstart,
+                           const int64_t *d_off, const int32_t *d_ind,
+                           int64_t total_n, int64_t total_nnz, int64_t *d_r,
+                           int64_t *d_t, double *d_lcc, int64_t *d_graph_T,
+                           void *d_workspace, size_t ws_bytes,
+                           const gtc_tuning *tuning, gtc_stream_t stream);
+
+/*
+ * Gather separate device-resident graphs (graph-local int64 offsets and int32
+ * ids; host arrays of their device pointers and sizes) into the batched
+ * layout above.  d_scratch needs gtc_batch_pack_scratch_bytes(G) bytes;
+ * h_staging is pinned host memory of the same size that must stay untouched
+ * until the stream has passed this call.
+ */
+size_t gtc_batch_pack_scratch_bytes(int64_t num_graphs);
+gtc_status gtc_batch_pack(int64_t num_graphs, const void *const *h_off,
+                          const void *const *h_ind, const int64_t *h_n,
+                          const int64_t *h_nnz, int64_t *d_vstart,
+                          int64_t *d_off, int32_t *d_ind, void *d_scratch,
+                          size_t scratch_bytes, void *h_staging,
+                          gtc_stream_t stream);
+
+/*
  * Check the CSR input contract on the device.  Synchronous: writes a
  * gtc_csr_reason to *h_reason and returns GTC_OK (the status reports only
  * call failures; an invalid graph is reported through *h_reason).

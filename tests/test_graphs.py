@@ -75,3 +75,25 @@ def test_to_device_roundtrip_cpu():
     g = G.cycle(6)
     h = g.to("cpu").numpy()
     assert np.array_equal(h.off, g.off) and torch.is_tensor(g.to("cpu").off)
+
+
+def test_batched_specs_shape():
+    specs = G.batched_specs(4096, 4)
+    ns = np.array([s["n"] for s in specs])
+    assert len(specs) == 4096 and ns.min() >= 256 and ns.max() <= 262_144
+    assert sum(s["kind"] == "er" for s in specs) == 2048
+    assert specs == G.batched_specs(4096, 4)
+    er = [s["mean_degree"] for s in specs if s["kind"] == "er"]
+    ef = [s["edge_factor"] for s in specs if s["kind"] == "rmat"]
+    assert 8 <= min(er) and max(er) <= 32 and 8 <= min(ef) and max(ef) <= 16
+
+
+def test_concat_and_slice_roundtrip():
+    gs = [G.make_spec_graph(s) for s in G.batched_specs(10, 3, 256, 2000)]
+    b = G.concat_graphs(gs, "cpu")
+    assert b.num_graphs == 10 and b.total_n == sum(g.n for g in gs)
+    for i, g in enumerate(gs):
+        h = b.graph(i)
+        assert np.array_equal(np.asarray(h.off), np.asarray(g.off))
+        assert np.array_equal(np.asarray(h.ind), np.asarray(g.ind))
+        assert G.validate_csr_host(np.asarray(h.off), np.asarray(h.ind)) is None
