@@ -43,6 +43,12 @@ CONFIGS = {
                label="Erdos-Renyi n=16384, mean degree 16, seed 1"),
     "rgg": dict(kind="rgg", n=1 << 22, deg=12, seed=3,
                 label="2D RGG n=4194304, mean degree 12, Morton order, seed 3"),
+    "serving": dict(kind="serving", pool=256, seed=5, rates=(1000, 5000, 20000),
+                    arrivals_s=1.5,
+                    label="Poisson arrivals at 1k, 5k and 20k requests/s; each request a graph "
+                          "from the batched-workload generator (pool of 256, seed 5) or, with "
+                          "probability 1%, an R-MAT scale 22 edge factor 16 graph; CSRs resident "
+                          "in HBM"),
     "batched": dict(kind="batched", graphs=4096, seed=4,
                     label="4,096 graphs, n log-uniform in [256, 262144], half ER (mean degree "
                           "U[8,32]), half R-MAT (0.57,0.19,0.19,0.05, edge factor U[8,16]), seed 4; "
@@ -187,8 +193,8 @@ def run_reference(args, cfg, rank: int) -> None:
     if rank != 0:
         return
     threads = O.max_threads()
-    if cfg["kind"] == "batched":
-        run_reference_batched(args, cfg, threads)
+    if cfg["kind"] in ("batched", "serving"):
+        run_reference_batched(args, CONFIGS["batched"], threads)
         return
     g = make_graph(cfg, "cpu").numpy()
     prep = O.ref_prepared(g.off, g.ind)
@@ -222,8 +228,9 @@ def run_reference(args, cfg, rank: int) -> None:
 
 def run_reference_batched(args, cfg, threads: int) -> None:
     """Reference CPU code on a bounded sample of the batched workload: every
-    64th graph (the same graphs the GPU arm counts, generated on the host),
-    each counted whole by the reference's vertex-list overload."""
+    64th graph spec (same generator and seeds as the GPU arm, realised with
+    the host RNG), each counted whole by the reference's vertex-list
+    overload."""
     from gputrianglecounting_b200 import graphs as G
     from oracle import oracle as O
     specs = G.batched_specs(cfg["graphs"], cfg["seed"])[::64]
@@ -526,6 +533,59 @@ def run_batched(args, cfg, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ serving
+
+def run_serving(args, cfg, rank: int, world: int) -> None:
+    """Continuous batching under Poisson load: p50/p99 latency and sustained
+    edges/s per arrival rate (each rank serves its own stream)."""
+    import torch
+    from gputrianglecounting_b200 import graphs as G, serve
+    from gputrianglecounting_b200._lib import load as load_lib
+    load_lib()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    specs = G.batched_specs(cfg["pool"], cfg["seed"])
+    pool = [G.make_spec_graph(s, dev) for s in specs]
+    big = [G.rmat(22, 16, cfg["seed"] * 10 + k, device=dev) for k in range(2)]
+    graphs = pool + big
+    torch.cuda.synchronize()
+    server = serve.CountServer(graphs, dev, slots=3, budget_bytes=4 << 30, max_graphs=512)
+    # warm-up: every graph once, to size the slots' workspaces
+    warm = [serve.Request(i, i, 0.0) for i in range(len(graphs))]
+    server.run(warm)
+    per_rate = {}
+    rng = np.random.default_rng(cfg["seed"])
+    with ClockSampler(local) as clk:
+        for rate in cfg["rates"]:
+            count = int(rate * cfg["arrivals_s"])
+            arr = serve.poisson_arrivals(float(rate), count, seed=cfg["seed"] + rate)
+            pick = rng.random(count) < 0.01
+            gid = np.where(pick, len(pool) + rng.integers(0, len(big), count),
+                           rng.integers(0, len(pool), count))
+            reqs = [serve.Request(i, int(g), float(t)) for i, (g, t) in enumerate(zip(gid, arr))]
+            server.batches = 0
+            done = server.run(reqs, timeout_s=300)
+            st = serve.latency_stats(done)
+            st["batches"] = server.batches
+            st["large_requests"] = int(pick.sum())
+            per_rate[str(rate)] = st
+    if rank != 0:
+        return
+    top = per_rate[str(cfg["rates"][-1])]
+    line = {
+        "metric": "serving sustained edges/s (p50/p99 latency per rate)",
+        "value": top["sustained_edges_per_s"] * world, "unit": UNIT, "n_gpus": world,
+        "steps": len(cfg["rates"]), "warmup": 1, "ms_per_step": top["p50_ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32 ids / int64 counts", "data": "synthetic",
+        "config": {"workload": "serving", "graph": cfg["label"], "slots": 3,
+                   "slot_budget_gb": 4, "max_graphs_per_batch": 512},
+        "serving": per_rate, "clocks": clk.result,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -553,6 +613,8 @@ def main() -> None:
     try:
         if args.config == "batched":
             run_batched(args, cfg, rank, world)
+        elif args.config == "serving":
+            run_serving(args, cfg, rank, world)
         else:
             run_b200(args, cfg, rank, world)
     finally:
