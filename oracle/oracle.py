@@ -9,6 +9,9 @@ bench.py's CPU-baseline / reference arm, never by the product package.
   unchanged (oracle/Makefile target `ref`) behind oracle/ref_cpu_shim.cpp.
 * _ref/libref_gpu.so -- the reference's own src/clusteringCount.cu compiled for
   sm_100a behind oracle/ref_gpu_shim.cu (GPU tests only, tpi = 1).
+* _ref/libref_formats.so -- the reference's METIS converter
+  (src/csrdatacreate.cpp) and `.info` reader (src/graphRead.cpp) behind
+  oracle/ref_formats_shim.cpp and oracle/ref_info_shim.cpp (format tests).
 """
 from __future__ import annotations
 
@@ -181,3 +184,39 @@ def ref_rows_prepared(off64, ind64, vertices64, tri, r, threads: int = 0) -> int
 
 def max_threads() -> int:
     return int(oracle_lib().oracle_max_threads())
+
+
+# ---------------------------------------------------------------- formats
+
+REF_FORMATS_SO = os.path.join(HERE, "_ref", "libref_formats.so")
+
+
+def ref_formats_available() -> bool:
+    return os.path.exists(REF_FORMATS_SO)
+
+
+def ref_formats_lib() -> ctypes.CDLL:
+    P = c_void_p
+    return _load(REF_FORMATS_SO, {
+        "ref_metis_to_info": (c_int64, [ctypes.c_char_p, ctypes.c_char_p, P]),
+        "ref_read_info": (c_int64, [ctypes.c_char_p, P, c_int64, P, c_int64, P]),
+    })
+
+
+def ref_metis_to_info(metis_path: str, info_path: str) -> int:
+    """The reference's own converter (src/csrdatacreate.cpp) writing .info."""
+    nnz = ctypes.c_int64(0)
+    return int(ref_formats_lib().ref_metis_to_info(metis_path.encode(), info_path.encode(),
+                                                    ctypes.byref(nnz)))
+
+
+def ref_read_info(base: str, cap_n: int, cap_nnz: int):
+    """The reference's own .info reader (src/graphRead.cpp); reads base + '.info'."""
+    off = np.zeros(cap_n + 1, np.int64)
+    ind = np.zeros(max(cap_nnz, 1), np.int64)
+    nnz = ctypes.c_int64(0)
+    n = ref_formats_lib().ref_read_info(base.encode(), off.ctypes.data_as(c_void_p), cap_n + 1,
+                                        ind.ctypes.data_as(c_void_p), cap_nnz, ctypes.byref(nnz))
+    if n < 0:
+        raise RuntimeError("buffers too small")
+    return off[:n + 1], ind[:nnz.value]
