@@ -390,9 +390,9 @@ def run_b200(args, cfg, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
-# degree, tile bounds, tile count, scan x3, tile fill, vinfo, scan x3, group
-# kernel, block kernel, finalize, global
-LAUNCHES_PER_COUNT = 15
+# degree, tile bounds, tile count, scan x3, tile fill, vinfo, scan x3, item
+# rows, warp kernel, block kernel, finalize, global
+LAUNCHES_PER_COUNT = 16
 
 
 def phase_breakdown(counter, g, flush) -> dict:
@@ -422,7 +422,7 @@ def phase_breakdown(counter, g, flush) -> dict:
 
 # ------------------------------------------------------------------ batched
 
-BATCH_LAUNCHES = 18   # entry starts, globalize, the 15-launch pipeline, per-graph T
+BATCH_LAUNCHES = 19   # entry starts, globalize, the 16-launch pipeline, per-graph T
 
 
 def run_batched(args, cfg, rank: int, world: int) -> None:

@@ -334,8 +334,9 @@ gtc_status gtc_count_tuned(const void *d_off, int off_bits, const int32_t *d_ind
                 return GTC_ERR_INVALID_ARGUMENT;
             cfg.group = tuning->group;
         }
-        if (tuning->item_len < 0 || tuning->big_chunk < 0 || tuning->big_hash_max < 0 ||
-            tuning->big_hash_max > kBigHashMaxFdeg)
+        if (tuning->item_len < 0 || (tuning->item_len > 0 && tuning->item_len < kMinItemLen) ||
+            tuning->big_chunk < 0 || tuning->big_hash_max < 0 ||
+            tuning->big_hash_max > kBigHashMaxFdeg || tuning->big_chunk > 32768)
             return GTC_ERR_INVALID_ARGUMENT;
         if (tuning->item_len) cfg.item_len = tuning->item_len;
         if (tuning->big_chunk) cfg.big_chunk = tuning->big_chunk;

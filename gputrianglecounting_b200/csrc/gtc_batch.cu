@@ -189,7 +189,8 @@ gtc_status gtc_count_batch(int64_t num_graphs, const int64_t *d_vstart, const in
                 return GTC_ERR_INVALID_ARGUMENT;
             cfg.group = tuning->group;
         }
-        if (tuning->item_len < 0 || tuning->big_chunk < 0 || tuning->big_hash_max < 0 ||
+        if (tuning->item_len < 0 || (tuning->item_len > 0 && tuning->item_len < kMinItemLen) ||
+            tuning->big_chunk < 0 || tuning->big_hash_max < 0 ||
             tuning->big_hash_max > kBigHashMaxFdeg || tuning->big_chunk > 32768)
             return GTC_ERR_INVALID_ARGUMENT;
         if (tuning->item_len) cfg.item_len = tuning->item_len;

@@ -439,6 +439,17 @@ __device__ __forceinline__ void flush_hits(const ApexTable &tab, int tsize, int 
     }
 }
 
+// First row of every warp work item (item k covers entries
+// [k*item_len, (k+1)*item_len)), all items at once, so no warp starts an item
+// with a dependent binary search.
+template <typename OffT>
+__global__ void item_rows_kernel(const OffT *__restrict__ off, long long n, long long item_len,
+                                 long long n_items, long long *__restrict__ irow)
+{
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n_items) irow[k] = row_of_entry(off, n, k * item_len);
+}
+
 // Shuffle co-rank: the lane i whose [incl_i - w_i, incl_i) holds f (incl is
 // this lane's inclusive prefix of a per-lane count; lanes with count 0 are
 // never returned for f < total).
@@ -502,13 +513,13 @@ __device__ __forceinline__ void region_insert(int *keys, int toff, int lg, int k
 //      credits both itself and its apex; the per-slot 16-bit hit counters
 //      credit the third vertices in one flush per region.
 template <bool PER_VERTEX, typename OffT>
-__global__ void __launch_bounds__(kRowThreads)
+__global__ void __launch_bounds__(kRowThreads, kRowMinBlocks)
 count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                   long long n, long long nnz, const VInfo *__restrict__ vinfo,
                   const int *__restrict__ find,
                   unsigned long long *__restrict__ tacc, Counters *ctr,
-                  unsigned int *status, long long n_items, int item_len,
-                  int small_cap)
+                  unsigned int *status, const long long *__restrict__ irow,
+                  long long n_items, int item_len, int small_cap)
 {
     constexpr int kWarps = kRowThreads / 32;
     __shared__ int s_keys[kWarps][kRowSlots];
@@ -525,7 +536,7 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
         if (item >= n_items) break;
         const long long e0 = item * item_len;
         const long long e1 = (e0 + item_len < nnz) ? e0 + item_len : nnz;
-        long long ra = row_of_entry(off, n, e0);
+        long long ra = irow[item];
         while (true) {
             // ---- 1. rows of this batch (lane = row ra + lane)
             const long long r = ra + lane;
@@ -835,6 +846,7 @@ Plan make_plan(long long n, long long nnz, int off_bits, bool per_vertex)
     p.o_tacc = take(per_vertex ? sizeof(unsigned long long) * (size_t)n : 0);
     p.o_big = take(sizeof(long long) * (size_t)(n + 1));
     p.o_trow = take(sizeof(long long) * (size_t)(p.n_tiles + 1));
+    p.o_irow = take(sizeof(long long) * (size_t)(div_up<long long>(nnz, kMinItemLen) + 1));
     p.bytes = o;
     return p;
 }
@@ -870,6 +882,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
     unsigned long long *tacc = reinterpret_cast<unsigned long long *>(base + p.o_tacc);
     long long *big = reinterpret_cast<long long *>(base + p.o_big);
     long long *trow = reinterpret_cast<long long *>(base + p.o_trow);
+    long long *irow = reinterpret_cast<long long *>(base + p.o_irow);
 
     int dev = 0;
     cudaGetDevice(&dev);
@@ -900,13 +913,16 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
         if (timing) cudaEventRecord(timing->ev[1], stream);
         if (nnz > 0) {
             const long long n_items = div_up<long long>(nnz, cfg.item_len);
+            item_rows_kernel<OffT><<<(unsigned)div_up<long long>(n_items, 256), 256, 0, stream>>>(
+                off, n, cfg.item_len, n_items, irow);
             auto launch_rows = [&](auto kern) {
                 int blocks = occupancy_blocks(kern, kRowThreads, 0, dev,
                                               &g_rows_blocks[dev & 63][per_vertex ? 1 : 0]);
                 long long need = div_up<long long>(n_items, kRowThreads / 32);
                 if (need < blocks) blocks = (int)need;
                 kern<<<blocks, kRowThreads, 0, stream>>>(off, ind, n, nnz, vinfo, find, tacc, ctr,
-                                                         status, n_items, cfg.item_len, small_cap);
+                                                         status, irow, n_items, cfg.item_len,
+                                                         small_cap);
             };
             if (per_vertex) launch_rows(count_rows_kernel<true, OffT>);
             else launch_rows(count_rows_kernel<false, OffT>);

@@ -32,7 +32,9 @@ constexpr int kPrepItemsPerThread = 8;      // (rows + entries) per thread
 constexpr int kPrepTile = kPrepThreads * kPrepItemsPerThread;
 
 constexpr int kRowThreads = 256;            // warp-per-item count kernel
-constexpr int kRowSlots = 1024;             // shared table slots per warp
+constexpr int kRowSlots = 512;              // shared table slots per warp
+constexpr int kRowMinBlocks = 6;            // 48 warps per SM (register budget 42)
+constexpr int kMinItemLen = 32;             // smallest warp work item (entries)
 constexpr int kBigThreads = 512;            // block-per-row count kernel
 constexpr int kBigTableLog2 = 13;
 constexpr int kBigTableSlots = 1 << kBigTableLog2;   // shared hash slots (block kernel)
@@ -100,7 +102,7 @@ struct Plan {
     // workspace byte offsets
     size_t o_status = 0, o_counters = 0, o_deg = 0, o_tile = 0, o_scan_tmp = 0,
            o_foff = 0, o_vinfo = 0, o_find = 0, o_tacc = 0, o_big = 0,
-           o_bigpre = 0, o_trow = 0;
+           o_bigpre = 0, o_trow = 0, o_irow = 0;
     size_t bytes = 0;
 };
 

@@ -102,8 +102,8 @@ gtc_status gtc_count(const void *d_off, int off_bits, const int32_t *d_ind,
  *   group        lanes that share one apex row in the group kernel: 4, 8,
  *                16 or 32; rows whose forward list is longer than
  *                4*group go to the block kernel
- *   item_len     adjacency entries per group-kernel work item
- *   big_chunk    adjacency entries per block-kernel work item
+ *   item_len     adjacency entries per warp work item (>= 32)
+ *   big_chunk    adjacency entries per block-kernel work item (<= 32768)
  *   big_hash_max longest forward list the block kernel hashes in shared
  *                memory (<= 2048); longer lists are binary-searched in place
  */
