@@ -127,10 +127,12 @@ __device__ __forceinline__ bool entry_forward(const TileSmem &s, long long li,
     return rank_above(deg[x], x, da, (int)a);
 }
 
-// Pass 1: number of forward entries per tile.
+// Pass 1, walking the items in order (one degree gather per entry): for
+// graphs whose neighbours are close in id and in cache, where the smaller
+// register footprint keeps more tiles resident.
 template <typename OffT>
 __global__ void __launch_bounds__(kPrepThreads)
-tile_count_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
+tile_count_seq_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                   const int *__restrict__ deg, long long n, long long nnz,
                   const long long *__restrict__ trow,
                   long long *__restrict__ tile_cnt, unsigned int *status)
@@ -164,12 +166,10 @@ tile_count_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
     }
 }
 
-// Pass 2: write the forward adjacency (ordered stream compaction of the
-// adjacency by the forward flag) and the forward offsets foff[r+1] at every
-// row end.
+// Pass 2, walking the items in order (see pass 1).
 template <typename OffT>
 __global__ void __launch_bounds__(kPrepThreads)
-tile_fill_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
+tile_fill_seq_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                  const int *__restrict__ deg, long long n, long long nnz,
                  const long long *__restrict__ trow,
                  const long long *__restrict__ tile_pre,
@@ -219,6 +219,137 @@ tile_fill_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
         } else {
             if (flags & (1u << k)) find[pos++] = s.ind[lj];
             ++lj;
+        }
+    }
+}
+
+// This thread's items of the staged tile, classified from shared memory
+// only: row ends and entries (with the entry's neighbour id and its row's
+// degree), so that the degree gathers of all entries can be issued at once.
+struct ThreadItems {
+    unsigned int entry_mask;                 // bit k: item k is an entry
+    unsigned int rowend_mask;                // bit k: item k ends a row
+    int x[kPrepItemsPerThread];              // neighbour id (entries)
+    int da[kPrepItemsPerThread];             // degree of the entry's row
+    int rowloc[kPrepItemsPerThread];         // local row index of the item
+};
+
+__device__ __forceinline__ void tile_classify(const TileSmem &s, ThreadItems &it)
+{
+    long long li, lj;
+    tile_thread_start(s, li, lj);
+    const long long rows = s.r1 - s.r0, ents = s.e1 - s.e0;
+    it.entry_mask = it.rowend_mask = 0;
+#pragma unroll
+    for (int k = 0; k < kPrepItemsPerThread; ++k) {
+        it.x[k] = 0;
+        it.da[k] = 0;
+        it.rowloc[k] = (int)li;
+        if (li + lj < rows + ents) {
+            if (li < rows && lj >= s.off[li + 1] - s.e0) {
+                it.rowend_mask |= 1u << k;
+                ++li;
+            } else {
+                it.entry_mask |= 1u << k;
+                it.x[k] = s.ind[lj];
+                it.da[k] = (int)(s.off[li + 1] - s.off[li]);
+                ++lj;
+            }
+        }
+    }
+}
+
+// Forward flags of the thread's entries (bit k for item k), with every
+// degree gather issued before any flag is computed (skewed graphs, whose
+// neighbour degrees are scattered over memory).
+__device__ __forceinline__ unsigned int forward_flags(const TileSmem &s, const ThreadItems &it,
+                                                      const int *__restrict__ deg, long long n,
+                                                      unsigned int *status)
+{
+    unsigned int flags = 0;
+    int dx[kPrepItemsPerThread];
+#pragma unroll
+    for (int k = 0; k < kPrepItemsPerThread; ++k) {
+        const bool ok = ((it.entry_mask >> k) & 1u) &&
+                        (unsigned long long)(long long)it.x[k] < (unsigned long long)n;
+        dx[k] = ok ? deg[it.x[k]] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kPrepItemsPerThread; ++k) {
+        if (!((it.entry_mask >> k) & 1u)) continue;
+        if ((unsigned long long)(long long)it.x[k] >= (unsigned long long)n) {
+            atomicOr(status, kErrIndexRange);
+            continue;
+        }
+        if (rank_above(dx[k], it.x[k], it.da[k], (int)(s.r0 + it.rowloc[k]))) flags |= 1u << k;
+    }
+    return flags;
+}
+
+// Pass 1: number of forward entries per tile (gather-first variant).
+template <typename OffT>
+__global__ void __launch_bounds__(kPrepThreads)
+tile_count_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
+                  const int *__restrict__ deg, long long n, long long nnz,
+                  const long long *__restrict__ trow,
+                  long long *__restrict__ tile_cnt, unsigned int *status)
+{
+    __shared__ TileSmem s;
+    __shared__ int warp_sum[kPrepThreads / 32];
+    tile_stage(s, off, ind, n, nnz, trow);
+    ThreadItems it;
+    tile_classify(s, it);
+    int w = __popc(forward_flags(s, it, deg, n, status));
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = w;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long t = 0;
+        for (int i = 0; i < kPrepThreads / 32; ++i) t += warp_sum[i];
+        tile_cnt[blockIdx.x] = t;
+    }
+}
+
+// Pass 2: write the forward adjacency (ordered stream compaction of the
+// adjacency by the forward flag) and the forward offsets foff[r+1] at every
+// row end (gather-first variant).
+template <typename OffT>
+__global__ void __launch_bounds__(kPrepThreads)
+tile_fill_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
+                 const int *__restrict__ deg, long long n, long long nnz,
+                 const long long *__restrict__ trow,
+                 const long long *__restrict__ tile_pre,
+                 long long *__restrict__ foff, int *__restrict__ find,
+                 unsigned int *status)
+{
+    __shared__ TileSmem s;
+    __shared__ int warp_sum[kPrepThreads / 32];
+    tile_stage(s, off, ind, n, nnz, trow);
+    ThreadItems it;
+    tile_classify(s, it);
+    const unsigned int flags = forward_flags(s, it, deg, n, status);
+    const int cnt = __popc(flags);
+    // block exclusive scan of cnt
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        int o = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += o;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    int wbase = 0;
+    for (int i = 0; i < warp; ++i) wbase += warp_sum[i];
+    long long pos = tile_pre[blockIdx.x] + wbase + incl - cnt;
+    if (blockIdx.x == 0 && threadIdx.x == 0) foff[0] = 0;
+#pragma unroll
+    for (int k = 0; k < kPrepItemsPerThread; ++k) {
+        if ((it.rowend_mask >> k) & 1u) {
+            foff[s.r0 + it.rowloc[k] + 1] = pos;    // the row ends here
+        } else if ((flags >> k) & 1u) {
+            find[pos++] = it.x[k];
         }
     }
 }
@@ -855,8 +986,8 @@ RowConfig pick_row_config(long long n, long long nnz)
 {
     RowConfig c;
     const double avg = n > 0 ? (double)nnz / (double)n : 0.0;
-    if (avg <= 24.0) { c.group = 8; c.item_len = 256; }
-    else { c.group = 32; c.item_len = 512; }
+    if (avg <= 24.0) { c.group = 8; c.item_len = 256; c.prep_gather = false; }
+    else { c.group = 32; c.item_len = 512; c.prep_gather = true; }
     c.big_chunk = 2048;
     return c;
 }
@@ -900,12 +1031,22 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
         degree_kernel<<<vb, 256, 0, stream>>>(off, off_bits, n, deg);
         tile_bounds_kernel<OffT><<<(unsigned)div_up<long long>(p.n_tiles + 1, 256), 256, 0,
                                    stream>>>(off, n, nnz, p.n_tiles, trow);
-        tile_count_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
-            off, ind, deg, n, nnz, trow, tile, status);
+        if (cfg.prep_gather) {
+            tile_count_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
+                off, ind, deg, n, nnz, trow, tile, status);
+        } else {
+            tile_count_seq_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
+                off, ind, deg, n, nnz, trow, tile, status);
+        }
         err = exclusive_scan_i64(tile, tile, p.n_tiles, scan_tmp, stream);
         if (err != cudaSuccess) return GTC_ERR_CUDA;
-        tile_fill_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
-            off, ind, deg, n, nnz, trow, tile, foff, find, status);
+        if (cfg.prep_gather) {
+            tile_fill_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
+                off, ind, deg, n, nnz, trow, tile, foff, find, status);
+        } else {
+            tile_fill_seq_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
+                off, ind, deg, n, nnz, trow, tile, foff, find, status);
+        }
         const int small_cap = 4 * cfg.group;   // <= kRowSlots / 8
         vinfo_kernel<<<vb, 256, 0, stream>>>(foff, deg, n, small_cap, cfg.big_chunk, vinfo, big);
         err = exclusive_scan_i64(big, big, n, scan_tmp, stream);
