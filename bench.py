@@ -266,10 +266,11 @@ def run_reference_batched(args, cfg, threads: int) -> None:
 
 # ------------------------------------------------------------------ b200
 
-def run_b200(args, cfg, rank: int, world: int) -> None:
+def run_b200(args, cfg, rank: int, world: int):
     import torch
     import torch.distributed as dist
     from gputrianglecounting_b200 import api
+    from gputrianglecounting_b200 import dist as gdist
     from gputrianglecounting_b200._lib import load as load_lib
     load_lib()
 
@@ -309,11 +310,7 @@ def run_b200(args, cfg, rank: int, world: int) -> None:
     if world > 1:
         dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = gdist.max_over_ranks(sum(step_ms), dev)
     T = out.triangles
 
     # phase breakdown of one count (events between the pipeline phases)
@@ -343,17 +340,13 @@ def run_b200(args, cfg, rank: int, world: int) -> None:
         if k >= args.warmup:
             e2e_evs[k - args.warmup][1].record(stream)
     torch.cuda.synchronize()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_evs)
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = gdist.max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_evs), dev)
     assert int(h_glob[0]) == T, "end-to-end result differs from the device-resident run"
     h2d = host.off.nbytes + host.ind.nbytes
     d2h = h_r.numel() * 8 + h_lcc.numel() * 8 + 3 * 8
 
     if rank != 0:
-        return
+        return None
     m = host.m
     edges_all = m * world * args.steps
     value = edges_all / (total_ms / 1e3)
@@ -387,7 +380,7 @@ def run_b200(args, cfg, rank: int, world: int) -> None:
     if not args.no_cpu_baseline:
         from oracle import oracle as O
         line["cpu_baseline"] = cpu_baseline(host, O.max_threads())
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # degree, tile bounds, tile count, scan x3, tile fill, vinfo, scan x3, item
@@ -425,12 +418,13 @@ def phase_breakdown(counter, g, flush) -> dict:
 BATCH_LAUNCHES = 19   # entry starts, globalize, the 16-launch pipeline, per-graph T
 
 
-def run_batched(args, cfg, rank: int, world: int) -> None:
+def run_batched(args, cfg, rank: int, world: int):
     """4,096 graphs: one persistent-pipeline run per step, replayed as a
     captured CUDA graph, against the same engine called once per graph."""
     import torch
     import torch.distributed as dist
     from gputrianglecounting_b200 import api, graphs as G
+    from gputrianglecounting_b200 import dist as gdist
     from gputrianglecounting_b200._lib import load as load_lib
     load_lib()
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -466,11 +460,7 @@ def run_batched(args, cfg, rank: int, world: int) -> None:
                 evs[k][1].record(stream)
         torch.cuda.synchronize()
     step_ms = sorted(a.elapsed_time(b) for a, b in evs)
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = gdist.max_over_ranks(sum(step_ms), dev)
     graph_T = out.graph_T.clone()
 
     # one call per graph, same engine, same outputs
@@ -495,7 +485,7 @@ def run_batched(args, cfg, rank: int, world: int) -> None:
     assert torch.equal(per_T, graph_T), "batched and per-graph counts differ"
     del graph
     if rank != 0:
-        return
+        return None
     value = m_total * world * args.steps / (total_ms / 1e3)
     base_value = m_total / (min(base_ms) / 1e3)
     p = lambda q: step_ms[min(len(step_ms) - 1, int(round(q * (len(step_ms) - 1))))]
@@ -530,12 +520,12 @@ def run_batched(args, cfg, rank: int, world: int) -> None:
                                 "kind": "reference",
                                 "sample": f"{len(sample)} of {len(graphs)} graphs (every 64th), "
                                           f"{m_s} edges in {dt:.2f} s"}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # ------------------------------------------------------------------ serving
 
-def run_serving(args, cfg, rank: int, world: int) -> None:
+def run_serving(args, cfg, rank: int, world: int):
     """Continuous batching under Poisson load: p50/p99 latency and sustained
     edges/s per arrival rate (each rank serves its own stream)."""
     import torch
@@ -571,7 +561,7 @@ def run_serving(args, cfg, rank: int, world: int) -> None:
             st["large_requests"] = int(pick.sum())
             per_rate[str(rate)] = st
     if rank != 0:
-        return
+        return None
     top = per_rate[str(cfg["rates"][-1])]
     line = {
         "metric": "serving sustained edges/s (p50/p99 latency per rate)",
@@ -583,7 +573,7 @@ def run_serving(args, cfg, rank: int, world: int) -> None:
                    "slot_budget_gb": 4, "max_graphs_per_batch": 512},
         "serving": per_rate, "clocks": clk.result,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main() -> None:
@@ -594,6 +584,8 @@ def main() -> None:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="rmat20")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload only: skip the batched and serving sub-runs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -612,11 +604,27 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
         if args.config == "batched":
-            run_batched(args, cfg, rank, world)
+            line = run_batched(args, cfg, rank, world)
         elif args.config == "serving":
-            run_serving(args, cfg, rank, world)
+            line = run_serving(args, cfg, rank, world)
         else:
-            run_b200(args, cfg, rank, world)
+            line = run_b200(args, cfg, rank, world)
+            if args.config == "rmat20" and not args.no_extras:
+                # the headline metric's other two parts: batched speedup and
+                # served latency, each from its own workload
+                sub = argparse.Namespace(**vars(args))
+                sub.steps, sub.warmup = 5, 3
+                b = run_batched(sub, CONFIGS["batched"], rank, world)
+                srv_cfg = dict(CONFIGS["serving"], arrivals_s=1.0)
+                sv = run_serving(sub, srv_cfg, rank, world)
+                if line is not None:
+                    line["batched"] = dict(b["batched"], workload=b["config"]["graph"],
+                                           graphs=b["config"]["graphs"], m=b["config"]["m"])
+                    if "cpu_baseline" in b:
+                        line["batched"]["cpu_baseline"] = b["cpu_baseline"]
+                    line["serving"] = dict(sv["serving"], workload=sv["config"]["graph"])
+        if line is not None:
+            print(json.dumps(line), flush=True)
     finally:
         if world > 1:
             import torch.distributed as dist

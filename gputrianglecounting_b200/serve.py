@@ -1,12 +1,15 @@
 """Continuous-batching count server on one GPU.
 
 Count requests arrive over time, each naming a graph whose CSR is already
-resident in HBM.  The server keeps a FIFO queue and a few *slots* (a CUDA
-stream, a batch workspace and output buffers each).  Whenever a slot is
-free it admits queued requests in arrival order while their combined device
-footprint fits the slot's memory budget (and the batch-size cap), packs
-their CSRs into the batched layout on the device (gtc_batch_pack) and counts
-them in one pipeline run (gtc_count_batch).  Requests that arrive while
+resident in HBM.  The server keeps two FIFO queues -- small and large
+requests (large: more than `large_nnz` adjacency entries) -- and a few
+*slots* (a CUDA stream, a batch workspace and output buffers each).
+Whenever a slot is free it admits queued small requests in arrival order
+while their combined device footprint fits the slot's memory budget (and the
+batch-size cap), packs their CSRs into the batched layout on the device
+(gtc_batch_pack) and counts them in one pipeline run (gtc_count_batch).  A
+large request runs alone, and large requests may hold at most all but one of
+the slots, so small requests never queue behind them.  Requests that arrive while
 batches run wait only for the next free slot, so admission and execution
 overlap.  Each result (T and the per-vertex r) stays on the device; its
 latency is the time from arrival to the host seeing the slot's completion
@@ -61,6 +64,21 @@ def plan_batch(queue, budget: int, max_graphs: int) -> int:
     return k
 
 
+def next_work(free_slot: bool, small_queue, large_queue, large_running: int,
+              slots: int) -> str:
+    """What a free slot takes next: "small" (a batch of small requests),
+    "large" (one large request) or "" (nothing).  Small requests go first;
+    large ones never take the last slot not already running a large one
+    (with a single slot they simply wait for an empty small queue)."""
+    if not free_slot:
+        return ""
+    if small_queue:
+        return "small"
+    if large_queue and large_running < max(1, slots - 1):
+        return "large"
+    return ""
+
+
 def poisson_arrivals(rate: float, count: int, seed: int) -> np.ndarray:
     """Arrival times (s) of a Poisson process with `rate` requests/s."""
     rng = np.random.default_rng(seed)
@@ -75,11 +93,13 @@ class _Slot:
     requests: list = field(default_factory=list)
     out: api.BatchCounts | None = None
     batch: api.BatchCSR | None = None
+    is_large: bool = False
 
 
 class CountServer:
     def __init__(self, graphs, device=None, slots: int = 3, budget_bytes: int = 6 << 30,
-                 max_graphs: int = 512, keep_vertex_results: bool = False):
+                 max_graphs: int = 512, keep_vertex_results: bool = False,
+                 large_nnz: int = 16 << 20):
         """graphs: device-resident CSRGraphs (int64 off, int32 ind) that
         requests refer to by index."""
         self.device = torch.device(device) if device is not None else torch.device(
@@ -90,7 +110,9 @@ class CountServer:
         self.keep = keep_vertex_results
         self.slots = [_Slot(torch.cuda.Stream(self.device), api.BatchCounter(self.device))
                       for _ in range(slots)]
-        self.queue: deque[Request] = deque()
+        self.queue: deque[Request] = deque()          # small requests
+        self.large: deque[Request] = deque()          # large requests
+        self.large_nnz = large_nnz
         self.batches = 0
 
     # ---- slots
@@ -103,6 +125,7 @@ class CountServer:
             ev = torch.cuda.Event()
             ev.record(slot.stream)
         slot.event, slot.requests, slot.out, slot.batch = ev, reqs, out, batch
+        slot.is_large = len(reqs) == 1 and reqs[0].nnz > self.large_nnz
         self.batches += 1
 
     def _finish(self, slot: _Slot, now: float) -> list[Request]:
@@ -132,15 +155,22 @@ class CountServer:
             if now > timeout_s:
                 raise TimeoutError(f"serving did not finish in {timeout_s} s")
             while pending and pending[0].arrival <= now:
-                self.queue.append(pending.popleft())
+                req = pending.popleft()
+                (self.large if req.nnz > self.large_nnz else self.queue).append(req)
             for slot in self.slots:
                 if slot.event is not None and slot.event.query():
                     finished += self._finish(slot, time.perf_counter() - t0)
             for slot in self.slots:
-                if slot.event is None and self.queue:
+                running_large = sum(1 for s in self.slots if s.event is not None and s.is_large)
+                what = next_work(slot.event is None, self.queue, self.large, running_large,
+                                 len(self.slots))
+                if what == "small":
                     k = plan_batch(self.queue, self.budget, self.max_graphs)
                     self._launch(slot, [self.queue.popleft() for _ in range(k)])
-            if not self.queue and pending and all(s.event is None for s in self.slots):
+                elif what == "large":
+                    self._launch(slot, [self.large.popleft()])
+            if (not self.queue and not self.large and pending
+                    and all(s.event is None for s in self.slots)):
                 # idle until the next arrival
                 wait = pending[0].arrival - (time.perf_counter() - t0)
                 if wait > 0:

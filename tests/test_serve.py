@@ -51,3 +51,12 @@ def test_served_results_equal_results_alone(cuda):
         assert torch.equal(r.r, rv)
     stats = serve.latency_stats(done)
     assert stats["p99_ms"] >= stats["p50_ms"] > 0
+
+
+def test_large_requests_never_take_the_last_slot():
+    q_small, q_large = [R(10, 100)], [R(10**6, 10**8)]
+    assert serve.next_work(True, q_small, q_large, 0, 3) == "small"
+    assert serve.next_work(True, [], q_large, 1, 3) == "large"
+    assert serve.next_work(True, [], q_large, 2, 3) == ""       # keep one slot for small ones
+    assert serve.next_work(False, q_small, q_large, 0, 3) == ""
+    assert serve.next_work(True, [], [], 0, 3) == ""
