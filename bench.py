@@ -56,6 +56,14 @@ CONFIGS = {
 }
 
 
+# DRAM bytes (read + write) of one complete count, summed over its 16 launches
+# from one ncu capture of this same workload (dram__bytes_read.sum +
+# dram__bytes_write.sum, cold L2 before each launch).  Far below B_alg: the
+# forward lists and the per-vertex records stay in the 126 MB L2, so most
+# probe reads never reach HBM.
+DRAM_TRAFFIC = {"rmat20": 1081080832, "rgg": 1402710528}
+
+
 def make_graph(cfg: dict, device):
     from gputrianglecounting_b200 import graphs as G
     if cfg["kind"] == "rmat":
@@ -365,7 +373,8 @@ def run_b200(args, cfg, rank: int, world: int):
                                                f"({L2_FLUSH_BYTES >> 20} MiB write)",
                    "parallelism": f"{world} independent replica(s)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": DRAM_TRAFFIC.get(args.config),
+                     "traffic_unit": "bytes per count (ncu capture of this workload)",
                      "scope": "one complete count (all launches of one gtc_count call)",
                      "work_model": f"B_alg = 4W + 4(n+1) + 4nnz + 16n = {work['B_alg']} bytes, "
                                    f"W = sum_undirected min(d_u, d_v) = {work['W']}",
