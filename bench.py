@@ -384,7 +384,7 @@ def run_b200(args, cfg, rank: int, world: int):
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms / args.steps},
         "clocks": clk.result,
-        "gpu_launches": LAUNCHES_PER_COUNT * args.steps,
+        "gpu_launches": launches_per_count(host.n, host.nnz) * args.steps,
     }
     if not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -392,9 +392,11 @@ def run_b200(args, cfg, rank: int, world: int):
     return line
 
 
-# degree, tile bounds, tile count, scan x3, tile fill, vinfo, scan x3, item
-# rows, warp kernel, block kernel, finalize, global
-LAUNCHES_PER_COUNT = 16
+def launches_per_count(n: int, nnz: int) -> int:
+    """Kernels of one plain count with every output (the library's own plan:
+    16 with vertex-id labels, 19 with degree-rank labels)."""
+    from gputrianglecounting_b200 import api
+    return api.launch_plan(n, nnz)["launches"]
 
 
 def phase_breakdown(counter, g, flush) -> dict:
@@ -424,7 +426,10 @@ def phase_breakdown(counter, g, flush) -> dict:
 
 # ------------------------------------------------------------------ batched
 
-BATCH_LAUNCHES = 19   # entry starts, globalize, the 16-launch pipeline, per-graph T
+def batch_launches(total_n: int, total_nnz: int) -> int:
+    """Entry starts + globalize + the pipeline without its global-count
+    kernel + per-graph T."""
+    return 2 + (launches_per_count(total_n, total_nnz) - 1) + 1
 
 
 def run_batched(args, cfg, rank: int, world: int):
@@ -513,7 +518,7 @@ def run_batched(args, cfg, rank: int, world: int):
                     "per_graph_ms": min(base_ms), "per_graph_edges_per_s": base_value,
                     "speedup_vs_one_call_per_graph": value / world / base_value},
         "clocks": clk.result,
-        "gpu_launches": BATCH_LAUNCHES * args.steps,
+        "gpu_launches": batch_launches(batch.total_n, batch.total_nnz) * args.steps,
     }
     if not args.no_cpu_baseline:
         from oracle import oracle as O

@@ -33,6 +33,7 @@ _SIGNATURES = {
     "gtc_count": (c_int, [P, c_int, P, c_int64, c_int64, c_int, P, P, P, P, P, c_size_t, P]),
     "gtc_count_tuned": (c_int, [P, c_int, P, c_int64, c_int64, c_int, P, P, P, P, P, c_size_t, P,
                                 P]),
+    "gtc_count_launches": (c_int, [c_int64, c_int64, c_int, P, P, P]),
     "gtc_count_phase_times": (c_int, [P, c_int, P, c_int64, c_int64, P, c_size_t, P]),
     "gtc_count_noalloc": (c_int, [P, c_int, P, c_int64, c_int64, c_int, P, P, P, P, P]),
     "gtc_batch_workspace_size": (c_int, [c_int64, c_int64, c_int64, P]),
@@ -58,7 +59,7 @@ _SIGNATURES = {
 class Tuning(ctypes.Structure):
     """gtc_tuning (0 = library choice)."""
     _fields_ = [("group", c_int), ("item_len", c_int), ("big_chunk", c_int),
-                ("big_hash_max", c_int)]
+                ("big_hash_max", c_int), ("labels", c_int)]
 
 
 _lib = None

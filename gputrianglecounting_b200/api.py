@@ -147,6 +147,23 @@ def count_triangles(off: torch.Tensor, ind: torch.Tensor, mode: str = "plain",
     return TriangleCounter(off.device).count(off, ind, mode=mode, outputs=outputs, stream=stream)
 
 
+LABELS = {1: "vertex-id", 2: "degree-rank"}
+
+
+def launch_plan(n: int, nnz: int, mode: str = "plain", tuning: dict | None = None) -> dict:
+    """What a count of an (n, nnz) graph would run, host-only: kernel launches
+    per count and the vertex labelling ("vertex-id" or "degree-rank")."""
+    if mode not in _MODES:
+        raise ValueError(f"mode must be one of {list(_MODES)}")
+    tun = _lib.Tuning(**{k: int(v) for k, v in tuning.items()}) if tuning else None
+    launches, labels = ctypes.c_int(0), ctypes.c_int(0)
+    check(_lib.load().gtc_count_launches(n, nnz, _MODES[mode],
+                                         ctypes.byref(tun) if tun is not None else None,
+                                         ctypes.byref(launches), ctypes.byref(labels)),
+          "gtc_count_launches")
+    return {"launches": launches.value, "labels": LABELS[labels.value]}
+
+
 def count_subset(off: torch.Tensor, ind: torch.Tensor, vertices: torch.Tensor,
                  stream=None) -> torch.Tensor:
     """r(v) for each listed vertex (the reference's vertex-list overload)."""

@@ -313,6 +313,20 @@ gtc_status gtc_workspace_size(int64_t n, int64_t nnz, int off_bits, gtc_mode mod
     return GTC_OK;
 }
 
+gtc_status gtc_count_launches(int64_t n, int64_t nnz, gtc_mode mode,
+                              const gtc_tuning *tuning, int *launches, int *labels)
+{
+    if (n < 0 || nnz < 0 || !launches || !labels ||
+        (mode != GTC_MODE_PLAIN && mode != GTC_MODE_ORIENTED))
+        return GTC_ERR_INVALID_ARGUMENT;
+    RowConfig cfg = pick_row_config(n, nnz);
+    const gtc_status st = apply_tuning(cfg, tuning);
+    if (st != GTC_OK) return st;
+    *launches = launches_per_count(cfg, mode == GTC_MODE_PLAIN);
+    *labels = cfg.rank_labels ? GTC_LABELS_DEGREE_RANK : GTC_LABELS_VERTEX_ID;
+    return GTC_OK;
+}
+
 gtc_status gtc_count_tuned(const void *d_off, int off_bits, const int32_t *d_ind, int64_t n,
                            int64_t nnz, gtc_mode mode, int64_t *d_r, int64_t *d_t,
                            double *d_lcc, int64_t *d_global, void *d_workspace, size_t ws_bytes,
@@ -327,21 +341,8 @@ gtc_status gtc_count_tuned(const void *d_off, int off_bits, const int32_t *d_ind
     if (ws_bytes < need) return GTC_ERR_WORKSPACE_TOO_SMALL;
     const bool pv = mode == GTC_MODE_PLAIN;
     RowConfig cfg = pick_row_config(n, nnz);
-    if (tuning) {
-        if (tuning->group) {
-            if (tuning->group != 4 && tuning->group != 8 && tuning->group != 16 &&
-                tuning->group != 32)
-                return GTC_ERR_INVALID_ARGUMENT;
-            cfg.group = tuning->group;
-        }
-        if (tuning->item_len < 0 || (tuning->item_len > 0 && tuning->item_len < kMinItemLen) ||
-            tuning->big_chunk < 0 || tuning->big_hash_max < 0 ||
-            tuning->big_hash_max > kBigHashMaxFdeg || tuning->big_chunk > 32768)
-            return GTC_ERR_INVALID_ARGUMENT;
-        if (tuning->item_len) cfg.item_len = tuning->item_len;
-        if (tuning->big_chunk) cfg.big_chunk = tuning->big_chunk;
-        if (tuning->big_hash_max) cfg.big_hash_max = tuning->big_hash_max;
-    }
+    st = apply_tuning(cfg, tuning);
+    if (st != GTC_OK) return st;
     long long *r = reinterpret_cast<long long *>(d_r);
     long long *t = reinterpret_cast<long long *>(d_t);
     long long *g = reinterpret_cast<long long *>(d_global);

@@ -182,21 +182,8 @@ gtc_status gtc_count_batch(int64_t num_graphs, const int64_t *d_vstart, const in
     const long long *off = reinterpret_cast<const long long *>(d_off);
 
     RowConfig cfg = pick_row_config(total_n, total_nnz);
-    if (tuning) {
-        if (tuning->group) {
-            if (tuning->group != 4 && tuning->group != 8 && tuning->group != 16 &&
-                tuning->group != 32)
-                return GTC_ERR_INVALID_ARGUMENT;
-            cfg.group = tuning->group;
-        }
-        if (tuning->item_len < 0 || (tuning->item_len > 0 && tuning->item_len < kMinItemLen) ||
-            tuning->big_chunk < 0 || tuning->big_hash_max < 0 ||
-            tuning->big_hash_max > kBigHashMaxFdeg || tuning->big_chunk > 32768)
-            return GTC_ERR_INVALID_ARGUMENT;
-        if (tuning->item_len) cfg.item_len = tuning->item_len;
-        if (tuning->big_chunk) cfg.big_chunk = tuning->big_chunk;
-        if (tuning->big_hash_max) cfg.big_hash_max = tuning->big_hash_max;
-    }
+    st = apply_tuning(cfg, tuning);
+    if (st != GTC_OK) return st;
 
     graph_entry_starts<<<(unsigned)div_up<long long>(num_graphs + 1, 256), 256, 0, s>>>(
         off, vstart, num_graphs, estart);

@@ -17,6 +17,11 @@ namespace gtc {
 
 // ======================================================= forward-list build
 
+__device__ __forceinline__ int rank_bucket(int d)
+{
+    return d < 0 ? 0 : (d < kRankBuckets ? d : kRankBuckets - 1);
+}
+
 __global__ void degree_kernel(const void *off_v, int off_bits, long long n,
                               int *__restrict__ deg)
 {
@@ -28,6 +33,120 @@ __global__ void degree_kernel(const void *off_v, int off_bits, long long n,
     } else {
         const long long *off = static_cast<const long long *>(off_v);
         deg[v] = (int)(off[v + 1] - off[v]);
+    }
+}
+
+// Degree of vertex v (0 past the end).
+__device__ __forceinline__ int vertex_degree(const void *off_v, int off_bits, long long n,
+                                             long long v)
+{
+    if (v >= n) return 0;
+    if (off_bits == 32) {
+        const int *off = static_cast<const int *>(off_v);
+        return off[v + 1] - off[v];
+    }
+    const long long *off = static_cast<const long long *>(off_v);
+    return (int)(off[v + 1] - off[v]);
+}
+
+// Count this block's kRankChunk vertices per degree bucket in shared memory
+// (warp-aggregated); v = base + k * kRankThreads + threadIdx.x.
+template <class Bucket>
+__device__ __forceinline__ void chunk_bucket_counts(unsigned int *cnt, long long n,
+                                                    const Bucket &bucket_of)
+{
+    for (int k = threadIdx.x; k < kRankBuckets; k += kRankThreads) cnt[k] = 0;
+    __syncthreads();
+    const long long base = (long long)blockIdx.x * kRankChunk;
+    const int lane = threadIdx.x & 31;
+#pragma unroll 4
+    for (int k = 0; k < kRankChunk / kRankThreads; ++k) {
+        const long long v = base + k * kRankThreads + threadIdx.x;
+        const unsigned int b = v < n ? (unsigned int)bucket_of(v) : 0xffffffffu;
+        const unsigned int peers = __match_any_sync(0xffffffffu, b);
+        if (v < n && lane == __ffs(peers) - 1) atomicAdd(&cnt[b], (unsigned int)__popc(peers));
+    }
+    __syncthreads();
+}
+
+// deg[v] and the degree-bucket histogram (rank labels): each block counts
+// kRankChunk vertices in shared memory and adds its non-zero buckets.
+__global__ void __launch_bounds__(kRankThreads)
+degree_hist_kernel(const void *off_v, int off_bits, long long n, int *__restrict__ deg,
+                   unsigned long long *__restrict__ hist)
+{
+    __shared__ unsigned int cnt[kRankBuckets];
+    chunk_bucket_counts(cnt, n, [&](long long v) {
+        const int d = vertex_degree(off_v, off_bits, n, v);
+        deg[v] = d;
+        return rank_bucket(d);
+    });
+    for (int k = threadIdx.x; k < kRankBuckets; k += kRankThreads)
+        if (cnt[k]) atomicAdd(&hist[k], (unsigned long long)cnt[k]);
+}
+
+// Exclusive scan of the degree-bucket histogram, in place (one block; each
+// thread owns kRankBuckets / kRankScanThreads consecutive buckets).
+__global__ void __launch_bounds__(kRankScanThreads)
+rank_scan_kernel(unsigned long long *__restrict__ hist)
+{
+    constexpr int kPer = kRankBuckets / kRankScanThreads;
+    __shared__ unsigned long long warp_sum[kRankScanThreads / 32];
+    unsigned long long h[kPer];
+    unsigned long long mine = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        h[k] = hist[threadIdx.x * kPer + k];
+        mine += h[k];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long incl = mine;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long o = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += o;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    unsigned long long run = incl - mine;
+    for (int i = 0; i < warp; ++i) run += warp_sum[i];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        hist[threadIdx.x * kPer + k] = run;
+        run += h[k];
+    }
+}
+
+// rank[v]: position of v in degree order (bucket start + arrival in the
+// bucket; ties between equal degrees fall in any order, which changes which
+// endpoint owns an edge but never a count); order[rank] = v.  Each block
+// reserves one range per non-zero bucket for its kRankChunk vertices, then
+// hands out positions from shared memory.
+__global__ void __launch_bounds__(kRankThreads)
+rank_kernel(const int *__restrict__ deg, long long n, unsigned long long *__restrict__ cursor,
+            int *__restrict__ rank, int *__restrict__ order)
+{
+    __shared__ unsigned int cnt[kRankBuckets];
+    chunk_bucket_counts(cnt, n, [&](long long v) { return rank_bucket(deg[v]); });
+    for (int k = threadIdx.x; k < kRankBuckets; k += kRankThreads)
+        if (cnt[k]) cnt[k] = (unsigned int)atomicAdd(&cursor[k], (unsigned long long)cnt[k]);
+    __syncthreads();
+    const long long base = (long long)blockIdx.x * kRankChunk;
+    const int lane = threadIdx.x & 31;
+#pragma unroll 4
+    for (int k = 0; k < kRankChunk / kRankThreads; ++k) {
+        const long long v = base + k * kRankThreads + threadIdx.x;
+        const unsigned int b = v < n ? (unsigned int)rank_bucket(deg[v]) : 0xffffffffu;
+        const unsigned int peers = __match_any_sync(0xffffffffu, b);
+        const int leader = __ffs(peers) - 1;
+        unsigned int at = 0;
+        if (v < n && lane == leader) at = atomicAdd(&cnt[b], (unsigned int)__popc(peers));
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (v < n) {
+            const int r = (int)(at + __popc(peers & ((1u << lane) - 1u)));
+            rank[v] = r;
+            order[r] = (int)v;
+        }
     }
 }
 
@@ -260,19 +379,24 @@ __device__ __forceinline__ void tile_classify(const TileSmem &s, ThreadItems &it
 }
 
 // Forward flags of the thread's entries (bit k for item k), with every
-// degree gather issued before any flag is computed (skewed graphs, whose
-// neighbour degrees are scattered over memory).
+// key gather issued before any flag is computed (skewed graphs, whose
+// neighbour keys are scattered over memory).  Degree keys (RANK = false):
+// an entry is forward when (deg x, x) > (deg row, row).  Rank keys: when
+// rank x > rank row; the gathered ranks are returned in rx for the fill.
+template <bool RANK>
 __device__ __forceinline__ unsigned int forward_flags(const TileSmem &s, const ThreadItems &it,
-                                                      const int *__restrict__ deg, long long n,
-                                                      unsigned int *status)
+                                                      const int *__restrict__ key, long long n,
+                                                      unsigned int *status,
+                                                      int (&rx)[kPrepItemsPerThread])
 {
     unsigned int flags = 0;
-    int dx[kPrepItemsPerThread];
+    int ra[kPrepItemsPerThread];
 #pragma unroll
     for (int k = 0; k < kPrepItemsPerThread; ++k) {
         const bool ok = ((it.entry_mask >> k) & 1u) &&
                         (unsigned long long)(long long)it.x[k] < (unsigned long long)n;
-        dx[k] = ok ? deg[it.x[k]] : 0;
+        rx[k] = ok ? key[it.x[k]] : 0;
+        ra[k] = (RANK && ok) ? key[s.r0 + it.rowloc[k]] : 0;
     }
 #pragma unroll
     for (int k = 0; k < kPrepItemsPerThread; ++k) {
@@ -281,16 +405,18 @@ __device__ __forceinline__ unsigned int forward_flags(const TileSmem &s, const T
             atomicOr(status, kErrIndexRange);
             continue;
         }
-        if (rank_above(dx[k], it.x[k], it.da[k], (int)(s.r0 + it.rowloc[k]))) flags |= 1u << k;
+        const bool fwd = RANK ? rx[k] > ra[k]
+                              : rank_above(rx[k], it.x[k], it.da[k], (int)(s.r0 + it.rowloc[k]));
+        if (fwd) flags |= 1u << k;
     }
     return flags;
 }
 
 // Pass 1: number of forward entries per tile (gather-first variant).
-template <typename OffT>
+template <typename OffT, bool RANK>
 __global__ void __launch_bounds__(kPrepThreads)
 tile_count_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
-                  const int *__restrict__ deg, long long n, long long nnz,
+                  const int *__restrict__ key, long long n, long long nnz,
                   const long long *__restrict__ trow,
                   long long *__restrict__ tile_cnt, unsigned int *status)
 {
@@ -299,7 +425,8 @@ tile_count_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
     tile_stage(s, off, ind, n, nnz, trow);
     ThreadItems it;
     tile_classify(s, it);
-    int w = __popc(forward_flags(s, it, deg, n, status));
+    int rx[kPrepItemsPerThread];
+    int w = __popc(forward_flags<RANK>(s, it, key, n, status, rx));
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
     if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = w;
@@ -313,11 +440,12 @@ tile_count_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
 
 // Pass 2: write the forward adjacency (ordered stream compaction of the
 // adjacency by the forward flag) and the forward offsets foff[r+1] at every
-// row end (gather-first variant).
-template <typename OffT>
+// row end (gather-first variant).  With rank keys the forward lists hold the
+// members' ranks (sorted afterwards by sort_lists_kernel).
+template <typename OffT, bool RANK>
 __global__ void __launch_bounds__(kPrepThreads)
 tile_fill_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
-                 const int *__restrict__ deg, long long n, long long nnz,
+                 const int *__restrict__ key, long long n, long long nnz,
                  const long long *__restrict__ trow,
                  const long long *__restrict__ tile_pre,
                  long long *__restrict__ foff, int *__restrict__ find,
@@ -328,7 +456,8 @@ tile_fill_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
     tile_stage(s, off, ind, n, nnz, trow);
     ThreadItems it;
     tile_classify(s, it);
-    const unsigned int flags = forward_flags(s, it, deg, n, status);
+    int rx[kPrepItemsPerThread];
+    const unsigned int flags = forward_flags<RANK>(s, it, key, n, status, rx);
     const int cnt = __popc(flags);
     // block exclusive scan of cnt
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -349,16 +478,119 @@ tile_fill_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
         if ((it.rowend_mask >> k) & 1u) {
             foff[s.r0 + it.rowloc[k] + 1] = pos;    // the row ends here
         } else if ((flags >> k) & 1u) {
-            find[pos++] = it.x[k];
+            find[pos++] = RANK ? rx[k] : it.x[k];
         }
+    }
+}
+
+// Sort one list of len <= 32*E ascending with the whole warp, in registers:
+// lane l holds elements l*E .. l*E+E-1 (padded with +infinity), bitonic
+// network with comparator distance j done inside a lane (j < E) or across
+// lanes by shuffle (j >= E).
+template <int E>
+__device__ __forceinline__ void warp_sort_regs(int *list, int len, int lane)
+{
+    int v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int i = lane * E + e;
+        v[e] = i < len ? list[i] : 0x7fffffff;
+    }
+#pragma unroll
+    for (int k = 2; k <= 32 * E; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= E) {
+                const int lj = j / E;
+                const bool lower = (lane & lj) == 0;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const bool asc = k >= E ? (lane & (k / E)) == 0 : (e & k) == 0;
+                    const int y = __shfl_xor_sync(0xffffffffu, v[e], lj);
+                    v[e] = (lower == asc) ? min(v[e], y) : max(v[e], y);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    if ((e & j) == 0) {
+                        const bool asc = k >= E ? (lane & (k / E)) == 0 : (e & k) == 0;
+                        const int a = v[e], b = v[e + j];
+                        v[e] = asc ? min(a, b) : max(a, b);
+                        v[e + j] = asc ? max(a, b) : min(a, b);
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int i = lane * E + e;
+        if (i < len) list[i] = v[e];
+    }
+}
+
+// Lists longer than kSortRegMax, sorted in place in global memory by the
+// warp: a bitonic sorter with ascending comparators only (the first step of
+// every merge size k compares i with its mirror in the k-block, the later
+// steps compare i with i + j).  Positions >= len hold +infinity implicitly:
+// a comparator that touches one never moves anything, so it is skipped.
+__device__ void warp_sort_global(int *list, int len, int lane)
+{
+    const int lp = ceil_log2(len);
+    const int half = 1 << (lp - 1);
+    for (int lk = 1; lk <= lp; ++lk) {
+        const int k = 1 << lk;
+        for (int lj = lk - 1; lj >= 0; --lj) {
+            const int j = 1 << lj;
+            const bool mirror = lj == lk - 1;
+            for (int t = lane; t < half; t += 32) {
+                const int lo = ((t >> lj) << (lj + 1)) | (t & (j - 1));
+                const int hi = mirror ? ((lo & ~(k - 1)) + (k - 1) - (lo & (k - 1))) : lo + j;
+                if (hi < len) {
+                    const int a = list[lo], b = list[hi];
+                    if (a > b) { list[lo] = b; list[hi] = a; }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Sort every forward list ascending (rank labels).  One warp per 32
+// consecutive rows, one list at a time: up to kSortRegMax elements in
+// registers, longer lists in place.
+__global__ void __launch_bounds__(kSortThreads)
+sort_lists_kernel(const long long *__restrict__ foff, long long n, int *__restrict__ find)
+{
+    const int lane = threadIdx.x & 31;
+    const long long v0 = ((long long)blockIdx.x * (kSortThreads / 32) + (threadIdx.x >> 5)) * 32;
+    if (v0 >= n) return;
+    const long long v = v0 + lane;
+    long long b = 0, e = 0;
+    if (v < n) { b = foff[v]; e = foff[v + 1]; }
+    unsigned int todo = __ballot_sync(0xffffffffu, e - b >= 2);
+    while (todo) {
+        const int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const long long lb = __shfl_sync(0xffffffffu, b, src);
+        const int len = (int)(__shfl_sync(0xffffffffu, e, src) - lb);
+        int *list = find + lb;
+        if (len <= 32) warp_sort_regs<1>(list, len, lane);
+        else if (len <= 64) warp_sort_regs<2>(list, len, lane);
+        else if (len <= 128) warp_sort_regs<4>(list, len, lane);
+        else if (len <= 256) warp_sort_regs<8>(list, len, lane);
+        else if (len <= 512) warp_sort_regs<16>(list, len, lane);
+        else if (len <= kSortRegMax) warp_sort_regs<32>(list, len, lane);
+        else warp_sort_global(list, len, lane);
+        __syncwarp();
     }
 }
 
 // Per-vertex record and block-kernel work: rows whose forward list exceeds
 // the group kernel's table get ceil(deg / big_chunk) block items.
 __global__ void vinfo_kernel(const long long *__restrict__ foff,
-                             const int *__restrict__ deg, long long n,
-                             int small_cap, int big_chunk,
+                             const int *__restrict__ deg, const int *__restrict__ rank,
+                             long long n, int small_cap, int big_chunk,
                              VInfo *__restrict__ vinfo,
                              long long *__restrict__ big_items)
 {
@@ -367,9 +599,10 @@ __global__ void vinfo_kernel(const long long *__restrict__ foff,
     VInfo r;
     r.fbeg = foff[v];
     r.fdeg = (int)(foff[v + 1] - r.fbeg);
-    r.deg = deg[v];
+    const int d = deg[v];
+    r.key = rank ? rank[v] : d;
     vinfo[v] = r;
-    big_items[v] = (r.fdeg > small_cap) ? div_up<long long>(r.deg, big_chunk) : 0;
+    big_items[v] = (r.fdeg > small_cap) ? div_up<long long>(d, big_chunk) : 0;
 }
 
 // ============================================================ intersection
@@ -443,15 +676,18 @@ __device__ __forceinline__ int sorted_find(const int *__restrict__ list,
 //   * the shorter lists are concatenated and swept G probes at a time, each
 //     lane finding its partner by a shuffle binary search over the work
 //     prefix (co-rank).
+// TRIM (rank labels, lists sorted ascending): an element ranked at or below
+// the apex (key ka) cannot be in N+(a), so it is never looked up, and a long
+// partner is swept from its end down to the first element at or below ka.
 // Partner credits: a long partner's hits are one warp reduction; a short
 // partner's hits are the popcount of each batch's hit ballot over the lanes
 // that batch gives it.
-//   lookup(w) -> slot >= 0 on a hit, -1 on a miss
+//   lookup(w) -> slot >= 0 on a hit, -1 on a miss (called with w > ka when TRIM)
 //   on_hit(slot, w): credit of the third vertex
 // Returns this lane's hit count (the apex credit).
-template <int G, bool PER_VERTEX, typename Grp, class Lookup, class OnHit>
+template <int G, bool PER_VERTEX, bool TRIM, typename Grp, class Lookup, class OnHit>
 __device__ __forceinline__ unsigned int
-probe_stride(const Grp &grp, long long s, long long end, int a, int da, int fa,
+probe_stride(const Grp &grp, long long s, long long end, int a, int ka, int fa,
              const int *__restrict__ ind, const VInfo *__restrict__ vinfo,
              const int *__restrict__ find, long long n,
              unsigned long long *__restrict__ tacc, unsigned int *status,
@@ -468,7 +704,7 @@ probe_stride(const Grp &grp, long long s, long long end, int a, int da, int fa,
             const VInfo ix = vinfo[x];
             fx = ix.fdeg;
             fbx = ix.fbeg;
-            const bool fwd = rank_above(ix.deg, x, da, a);
+            const bool fwd = rank_above(ix.key, x, ka, a);
             partner = fx > 0 && (fwd ? fx <= fa : fx < fa);
         } else {
             atomicOr(status, kErrIndexRange);
@@ -485,27 +721,48 @@ probe_stride(const Grp &grp, long long s, long long end, int a, int da, int fa,
         const int len = grp.shfl(fx, src);
         const int px = grp.shfl(x, src);
         unsigned int hx = 0;
-        int j = lane;
-        for (; j + G < len; j += 2 * G) {
-            const int w0 = list[j];
-            const int w1 = list[j + G];
-            const int s0 = lookup(w0);
-            const int s1 = lookup(w1);
-            if (s0 >= 0) {
-                ++hx;
-                if (PER_VERTEX) on_hit(s0, w0);
+        if (TRIM) {
+            for (int top = len; top > 0; top -= 2 * G) {
+                const int j0 = top - G + lane, j1 = top - 2 * G + lane;
+                const int w0 = j0 >= 0 ? list[j0] : ka;
+                const int w1 = j1 >= 0 ? list[j1] : ka;
+                const int s0 = w0 > ka ? lookup(w0) : -1;
+                const int s1 = w1 > ka ? lookup(w1) : -1;
+                if (s0 >= 0) {
+                    ++hx;
+                    if (PER_VERTEX) on_hit(s0, w0);
+                }
+                if (s1 >= 0) {
+                    ++hx;
+                    if (PER_VERTEX) on_hit(s1, w1);
+                }
+                // sorted: once a loaded element is at or below ka, so is
+                // every element before it (lanes past the list start load ka)
+                if (grp.any(w1 <= ka)) break;
             }
-            if (s1 >= 0) {
-                ++hx;
-                if (PER_VERTEX) on_hit(s1, w1);
+        } else {
+            int j = lane;
+            for (; j + G < len; j += 2 * G) {
+                const int w0 = list[j];
+                const int w1 = list[j + G];
+                const int s0 = lookup(w0);
+                const int s1 = lookup(w1);
+                if (s0 >= 0) {
+                    ++hx;
+                    if (PER_VERTEX) on_hit(s0, w0);
+                }
+                if (s1 >= 0) {
+                    ++hx;
+                    if (PER_VERTEX) on_hit(s1, w1);
+                }
             }
-        }
-        if (j < len) {
-            const int w0 = list[j];
-            const int s0 = lookup(w0);
-            if (s0 >= 0) {
-                ++hx;
-                if (PER_VERTEX) on_hit(s0, w0);
+            if (j < len) {
+                const int w0 = list[j];
+                const int s0 = lookup(w0);
+                if (s0 >= 0) {
+                    ++hx;
+                    if (PER_VERTEX) on_hit(s0, w0);
+                }
             }
         }
         if (PER_VERTEX) {
@@ -535,7 +792,7 @@ probe_stride(const Grp &grp, long long s, long long end, int a, int da, int fa,
         bool hit = false;
         if (f < total) {
             const int w = find[fb_i + (f - ex_i)];
-            const int slot = lookup(w);
+            const int slot = (!TRIM || w > ka) ? lookup(w) : -1;
             if (slot >= 0) {
                 hit = true;
                 if (PER_VERTEX) on_hit(slot, w);
@@ -554,18 +811,26 @@ probe_stride(const Grp &grp, long long s, long long end, int a, int da, int fa,
     return hits;
 }
 
-// Credit every third vertex w hit in this table (once per (apex, w)) and
-// return nothing; threads [t0, t0 + step) cover the table.
-template <typename T>
+// Label of a forward-list member -> vertex id (rank labels map through
+// order[]; vertex-id labels are the id).
+__device__ __forceinline__ int label_vertex(const int *__restrict__ order, int w)
+{
+    return order ? order[w] : w;
+}
+
+// Credit every third vertex w hit in this table (once per (apex, w));
+// threads [t0, t0 + step) cover the table.
 __device__ __forceinline__ void flush_hits(const ApexTable &tab, int tsize, int t0, int step,
-                                          unsigned long long *__restrict__ tacc)
+                                           unsigned long long *__restrict__ tacc,
+                                           const int *__restrict__ order)
 {
     for (int wd = t0; wd < (tsize >> 1); wd += step) {
         const unsigned int pair = tab.hit_pair(wd);
         if (pair) {
             const unsigned int lo = pair & 0xffffu, hi = pair >> 16;
-            if (lo) atomicAdd(&tacc[tab.keys[2 * wd]], (unsigned long long)lo);
-            if (hi) atomicAdd(&tacc[tab.keys[2 * wd + 1]], (unsigned long long)hi);
+            if (lo) atomicAdd(&tacc[label_vertex(order, tab.keys[2 * wd])], (unsigned long long)lo);
+            if (hi) atomicAdd(&tacc[label_vertex(order, tab.keys[2 * wd + 1])],
+                              (unsigned long long)hi);
         }
     }
 }
@@ -650,7 +915,8 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                   const int *__restrict__ find,
                   unsigned long long *__restrict__ tacc, Counters *ctr,
                   unsigned int *status, const long long *__restrict__ irow,
-                  long long n_items, int item_len, int small_cap)
+                  long long n_items, int item_len, int small_cap,
+                  const int *__restrict__ order)
 {
     constexpr int kWarps = kRowThreads / 32;
     __shared__ int s_keys[kWarps][kRowSlots];
@@ -722,7 +988,7 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                     const long long s0_i = __shfl_sync(0xffffffffu, s0, i);
                     const int ex_i = __shfl_sync(0xffffffffu, lexcl, i);
                     const int fa_i = __shfl_sync(0xffffffffu, vi.fdeg, i);
-                    const int da_i = __shfl_sync(0xffffffffu, vi.deg, i);
+                    const int ka_i = __shfl_sync(0xffffffffu, vi.key, i);
                     const int to_i = __shfl_sync(0xffffffffu, toff, i);
                     const int lg_i = __shfl_sync(0xffffffffu, lg, i);
                     const int a = (int)(ra + i);
@@ -735,7 +1001,7 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                             const VInfo ix = vinfo[x];
                             fx = ix.fdeg;
                             fbx = ix.fbeg;
-                            const bool fwd = rank_above(ix.deg, x, da_i, a);
+                            const bool fwd = rank_above(ix.key, x, ka_i, a);
                             partner = fx > 0 && (fwd ? fx <= fa_i : fx < fa_i);
                         } else {
                             atomicOr(status, kErrIndexRange);
@@ -782,8 +1048,10 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                         const unsigned int pair = hitw[k];
                         if (pair) {
                             const unsigned int lo = pair & 0xffffu, hi = pair >> 16;
-                            if (lo) atomicAdd(&tacc[keys[2 * k]], (unsigned long long)lo);
-                            if (hi) atomicAdd(&tacc[keys[2 * k + 1]], (unsigned long long)hi);
+                            if (lo) atomicAdd(&tacc[label_vertex(order, keys[2 * k])],
+                                              (unsigned long long)lo);
+                            if (hi) atomicAdd(&tacc[label_vertex(order, keys[2 * k + 1])],
+                                              (unsigned long long)hi);
                         }
                     }
                 }
@@ -802,20 +1070,28 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
     if (lane == 0 && tri_local) atomicAdd(&ctr->tri_total, tri_local);
 }
 
-// Block-per-row kernel for apexes whose forward list exceeds small_cap: the
-// whole block shares one table of up to kBigTableSlots slots (load factor
-// <= 1/8 up to kBigTableSlots/8 keys, <= 1/4 up to kBigHashMaxFdeg);
-// beyond big_hash_max the apex list is binary-searched in global memory.
+// Block-per-row kernel for apexes whose forward list exceeds small_cap.
+// Vertex-id labels: the whole block shares one hash table of up to
+// kBigTableSlots slots (load factor <= 1/8 up to kBigTableSlots/8 keys,
+// <= 1/4 up to kBigHashMaxFdeg); beyond big_hash_max the apex list is
+// binary-searched in global memory.
+// Rank labels: N+(a) lies in the ranks above the apex, (ka, n), so when that
+// range has at most 32*kBitWords ranks the block marks the apex's list in a
+// shared bitmap over it -- one load and one bit test per probe, no
+// collisions -- and keeps per 32-bit word the number of marked ranks below it
+// (pre), so a hit at rank w has index pre + popcount(lower bits of its word)
+// in the sorted apex list, which indexes its 16-bit hit counter.  Larger
+// ranges use the hash table or the binary search, with the rank keys.
 // Within an item the warps take 32-entry strides from a shared counter, so
 // uneven partner work does not idle the block at its barriers.
-template <bool PER_VERTEX, typename OffT>
+template <bool PER_VERTEX, typename OffT, bool RANK>
 __global__ void __launch_bounds__(kBigThreads)
 count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                  long long n, const VInfo *__restrict__ vinfo,
                  const int *__restrict__ find,
                  unsigned long long *__restrict__ tacc, Counters *ctr,
                  unsigned int *status, const long long *__restrict__ big_pre,
-                 int big_chunk, int big_hash_max)
+                 int big_chunk, int big_hash_max, const int *__restrict__ order)
 {
     extern __shared__ int smem[];
     int *keys = smem;
@@ -823,6 +1099,7 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
     __shared__ long long s_item;
     __shared__ unsigned int s_cnt;
     __shared__ int s_next;
+    __shared__ unsigned int s_wsum[kBigThreads / 32];
     auto block = cg::this_thread_block();
     auto warp = cg::tiled_partition<32>(block);
     const int lane = warp.thread_rank();
@@ -844,14 +1121,74 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
         long long re = rb + big_chunk;
         if (re > (long long)off[a + 1]) re = off[a + 1];
         const VInfo ia = vinfo[a];
-        const int fa = ia.fdeg;
+        const int fa = ia.fdeg, ka = ia.key;
+        const int *alist = find + ia.fbeg;
         unsigned int cnt = 0;
         auto next_stride = [&]() {
             int st = 0;
             if (lane == 0) st = atomicAdd(&s_next, 1);
             return rb + 32ll * warp.shfl(st, 0);
         };
-        if (fa <= big_hash_max) {
+        const long long range = RANK ? n - 1 - (long long)ka : 0;
+        if (RANK && range <= 32ll * kBitWords && fa <= kBitKeys) {
+            unsigned int *bits = reinterpret_cast<unsigned int *>(smem);
+            unsigned short *pre = reinterpret_cast<unsigned short *>(bits + kBitWords);
+            const int words = (int)((range + 31) >> 5);
+            for (int k = threadIdx.x; k < words; k += kBigThreads) bits[k] = 0;
+            if (PER_VERTEX)
+                for (int k = threadIdx.x; k < ((fa + 1) >> 1); k += kBigThreads) hitw[k] = 0;
+            __syncthreads();
+            for (int k = threadIdx.x; k < fa; k += kBigThreads) {
+                const unsigned int p = (unsigned int)(alist[k] - ka - 1);
+                atomicOr(&bits[p >> 5], 1u << (p & 31u));
+            }
+            __syncthreads();
+            if (PER_VERTEX) {
+                constexpr int kPer = kBitWords / kBigThreads;
+                const int w0 = threadIdx.x * kPer;
+                unsigned int c = 0;
+#pragma unroll
+                for (int k = 0; k < kPer; ++k) c += (w0 + k < words) ? __popc(bits[w0 + k]) : 0u;
+                unsigned int incl = c;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const unsigned int o = __shfl_up_sync(0xffffffffu, incl, d);
+                    if (lane >= d) incl += o;
+                }
+                if (lane == 31) s_wsum[threadIdx.x >> 5] = incl;
+                __syncthreads();
+                unsigned int run = incl - c;
+                for (int i = 0; i < (int)(threadIdx.x >> 5); ++i) run += s_wsum[i];
+#pragma unroll
+                for (int k = 0; k < kPer; ++k) {
+                    if (w0 + k < words) {
+                        pre[w0 + k] = (unsigned short)run;
+                        run += __popc(bits[w0 + k]);
+                    }
+                }
+                __syncthreads();
+            }
+            auto lookup = [bits, pre, ka](int w) -> int {
+                const unsigned int p = (unsigned int)(w - ka - 1);
+                const unsigned int word = bits[p >> 5];
+                const unsigned int b = p & 31u;
+                if (!((word >> b) & 1u)) return -1;
+                return PER_VERTEX ? (int)pre[p >> 5] + __popc(word & ((1u << b) - 1u)) : 0;
+            };
+            auto on_hit = [hitw](int slot, int) {
+                atomicAdd(&hitw[slot >> 1], 1u << ((slot & 1) << 4));
+            };
+            for (long long s = next_stride(); s < re; s = next_stride())
+                cnt += probe_stride<32, PER_VERTEX, true>(warp, s, re, (int)a, ka, fa, ind, vinfo,
+                                                          find, n, tacc, status, lookup, on_hit);
+            __syncthreads();
+            if (PER_VERTEX) {
+                for (int k = threadIdx.x; k < fa; k += kBigThreads) {
+                    const unsigned int c = (hitw[k >> 1] >> ((k & 1) << 4)) & 0xffffu;
+                    if (c) atomicAdd(&tacc[order[alist[k]]], (unsigned long long)c);
+                }
+            }
+        } else if (fa <= big_hash_max) {
             const int log2t = min(max(ceil_log2(8 * (long long)fa), 6), kBigTableLog2);
             const int tsize = 1 << log2t;
             for (int k = threadIdx.x; k < tsize; k += kBigThreads) keys[k] = -1;
@@ -859,24 +1196,23 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                 for (int k = threadIdx.x; k < (tsize >> 1); k += kBigThreads) hitw[k] = 0;
             __syncthreads();
             const ApexTable tab{keys, hitw, log2t, (unsigned int)(tsize - 1)};
-            for (int k = threadIdx.x; k < fa; k += kBigThreads) tab.insert(find[ia.fbeg + k]);
+            for (int k = threadIdx.x; k < fa; k += kBigThreads) tab.insert(alist[k]);
             __syncthreads();
             auto lookup = [tab](int w) { return tab.find(w); };
             auto on_hit = [tab](int slot, int) { tab.add_hit(slot); };
             for (long long s = next_stride(); s < re; s = next_stride())
-                cnt += probe_stride<32, PER_VERTEX>(warp, s, re, (int)a, ia.deg, fa, ind,
-                                                    vinfo, find, n, tacc, status, lookup,
-                                                    on_hit);
+                cnt += probe_stride<32, PER_VERTEX, RANK>(warp, s, re, (int)a, ka, fa, ind, vinfo,
+                                                          find, n, tacc, status, lookup, on_hit);
             __syncthreads();
-            if (PER_VERTEX) flush_hits<int>(tab, tsize, threadIdx.x, kBigThreads, tacc);
+            if (PER_VERTEX) flush_hits(tab, tsize, threadIdx.x, kBigThreads, tacc, order);
         } else {
-            const int *list = find + ia.fbeg;
-            auto lookup = [list, fa](int w) { return sorted_find(list, fa, w); };
-            auto on_hit = [tacc](int, int w) { atomicAdd(&tacc[w], 1ull); };
+            auto lookup = [alist, fa](int w) { return sorted_find(alist, fa, w); };
+            auto on_hit = [tacc, order](int, int w) {
+                atomicAdd(&tacc[label_vertex(order, w)], 1ull);
+            };
             for (long long s = next_stride(); s < re; s = next_stride())
-                cnt += probe_stride<32, PER_VERTEX>(warp, s, re, (int)a, ia.deg, fa, ind,
-                                                    vinfo, find, n, tacc, status, lookup,
-                                                    on_hit);
+                cnt += probe_stride<32, PER_VERTEX, RANK>(warp, s, re, (int)a, ka, fa, ind, vinfo,
+                                                          find, n, tacc, status, lookup, on_hit);
         }
         const unsigned int wsum = cg::reduce(warp, cnt, cg::plus<unsigned int>());
         if (lane == 0 && wsum) atomicAdd(&s_cnt, wsum);
@@ -926,7 +1262,7 @@ namespace {
 
 int g_sm_count[64];
 int g_rows_blocks[64][8];
-int g_big_blocks[64][2];
+int g_big_blocks[64][4];
 
 int device_sm_count(int dev)
 {
@@ -967,7 +1303,10 @@ Plan make_plan(long long n, long long nnz, int off_bits, bool per_vertex)
     auto take = [&](size_t bytes) { size_t at = o; o = align256(o + bytes); return at; };
     p.o_status = take(sizeof(unsigned int));
     p.o_counters = take(sizeof(Counters));
+    p.o_hist = take(sizeof(unsigned long long) * (size_t)kRankBuckets);
     p.o_deg = take(sizeof(int) * (size_t)n);
+    p.o_rank = take(sizeof(int) * (size_t)n);
+    p.o_order = take(sizeof(int) * (size_t)n);
     p.o_tile = take(sizeof(long long) * (size_t)(p.n_tiles + 1));
     long long scan_n = p.n_tiles > n ? p.n_tiles : n;
     p.o_scan_tmp = take(scan_tmp_bytes(scan_n));
@@ -986,10 +1325,43 @@ RowConfig pick_row_config(long long n, long long nnz)
 {
     RowConfig c;
     const double avg = n > 0 ? (double)nnz / (double)n : 0.0;
-    if (avg <= 24.0) { c.group = 8; c.item_len = 256; c.prep_gather = false; }
-    else { c.group = 32; c.item_len = 512; c.prep_gather = true; }
+    if (avg <= 24.0) {
+        c.group = 8; c.item_len = 256; c.prep_gather = false; c.rank_labels = false;
+    } else {
+        c.group = 32; c.item_len = 512; c.prep_gather = true; c.rank_labels = true;
+    }
     c.big_chunk = 2048;
     return c;
+}
+
+gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
+{
+    if (!tuning) return GTC_OK;
+    if (tuning->group) {
+        if (tuning->group != 4 && tuning->group != 8 && tuning->group != 16 &&
+            tuning->group != 32)
+            return GTC_ERR_INVALID_ARGUMENT;
+        cfg.group = tuning->group;
+    }
+    if (tuning->item_len < 0 || (tuning->item_len > 0 && tuning->item_len < kMinItemLen) ||
+        tuning->big_chunk < 0 || tuning->big_hash_max < 0 ||
+        tuning->big_hash_max > kBigHashMaxFdeg || tuning->big_chunk > 32768 ||
+        tuning->labels < 0 || tuning->labels > 2)
+        return GTC_ERR_INVALID_ARGUMENT;
+    if (tuning->item_len) cfg.item_len = tuning->item_len;
+    if (tuning->big_chunk) cfg.big_chunk = tuning->big_chunk;
+    if (tuning->big_hash_max) cfg.big_hash_max = tuning->big_hash_max;
+    if (tuning->labels == GTC_LABELS_VERTEX_ID) cfg.rank_labels = false;
+    if (tuning->labels == GTC_LABELS_DEGREE_RANK) cfg.rank_labels = true;
+    return GTC_OK;
+}
+
+int launches_per_count(const RowConfig &cfg, bool per_vertex)
+{
+    // degree, tile bounds, tile count, scan x3, tile fill, vinfo, scan x3,
+    // item rows, warp kernel, block kernel, global; finalize (per vertex);
+    // rank scan, rank, list sort (rank labels)
+    return 15 + (per_vertex ? 1 : 0) + (cfg.rank_labels ? 3 : 0);
 }
 
 template <typename OffT>
@@ -1014,12 +1386,16 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
     long long *big = reinterpret_cast<long long *>(base + p.o_big);
     long long *trow = reinterpret_cast<long long *>(base + p.o_trow);
     long long *irow = reinterpret_cast<long long *>(base + p.o_irow);
+    const bool rank_labels = cfg.rank_labels;
+    unsigned long long *hist = reinterpret_cast<unsigned long long *>(base + p.o_hist);
+    int *rank = reinterpret_cast<int *>(base + p.o_rank);
+    int *order = reinterpret_cast<int *>(base + p.o_order);
 
     int dev = 0;
     cudaGetDevice(&dev);
     cudaError_t err;
-    // status word and counters are adjacent at the start of the workspace
-    err = cudaMemsetAsync(base, 0, p.o_deg, stream);
+    // status word, counters (and the rank histogram) lead the workspace
+    err = cudaMemsetAsync(base, 0, rank_labels ? p.o_deg : p.o_hist, stream);
     if (err != cudaSuccess) return GTC_ERR_CUDA;
     if (per_vertex && n > 0) {
         err = cudaMemsetAsync(tacc, 0, sizeof(unsigned long long) * (size_t)n, stream);
@@ -1028,30 +1404,48 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
     if (n > 0) {
         const unsigned vb = (unsigned)div_up<long long>(n, 256);
         if (timing) cudaEventRecord(timing->ev[0], stream);
-        degree_kernel<<<vb, 256, 0, stream>>>(off, off_bits, n, deg);
+        if (rank_labels) {
+            const unsigned rb = (unsigned)div_up<long long>(n, kRankChunk);
+            degree_hist_kernel<<<rb, kRankThreads, 0, stream>>>(off, off_bits, n, deg, hist);
+            rank_scan_kernel<<<1, kRankScanThreads, 0, stream>>>(hist);
+            rank_kernel<<<rb, kRankThreads, 0, stream>>>(deg, n, hist, rank, order);
+        } else {
+            degree_kernel<<<vb, 256, 0, stream>>>(off, off_bits, n, deg);
+        }
         tile_bounds_kernel<OffT><<<(unsigned)div_up<long long>(p.n_tiles + 1, 256), 256, 0,
                                    stream>>>(off, n, nnz, p.n_tiles, trow);
-        if (cfg.prep_gather) {
-            tile_count_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
+        const unsigned nt = (unsigned)p.n_tiles;
+        if (rank_labels) {
+            tile_count_kernel<OffT, true><<<nt, kPrepThreads, 0, stream>>>(
+                off, ind, rank, n, nnz, trow, tile, status);
+        } else if (cfg.prep_gather) {
+            tile_count_kernel<OffT, false><<<nt, kPrepThreads, 0, stream>>>(
                 off, ind, deg, n, nnz, trow, tile, status);
         } else {
-            tile_count_seq_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
+            tile_count_seq_kernel<OffT><<<nt, kPrepThreads, 0, stream>>>(
                 off, ind, deg, n, nnz, trow, tile, status);
         }
         err = exclusive_scan_i64(tile, tile, p.n_tiles, scan_tmp, stream);
         if (err != cudaSuccess) return GTC_ERR_CUDA;
-        if (cfg.prep_gather) {
-            tile_fill_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
+        if (rank_labels) {
+            tile_fill_kernel<OffT, true><<<nt, kPrepThreads, 0, stream>>>(
+                off, ind, rank, n, nnz, trow, tile, foff, find, status);
+            sort_lists_kernel<<<(unsigned)div_up<long long>(n, 32 * (kSortThreads / 32)),
+                                kSortThreads, 0, stream>>>(foff, n, find);
+        } else if (cfg.prep_gather) {
+            tile_fill_kernel<OffT, false><<<nt, kPrepThreads, 0, stream>>>(
                 off, ind, deg, n, nnz, trow, tile, foff, find, status);
         } else {
-            tile_fill_seq_kernel<OffT><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
+            tile_fill_seq_kernel<OffT><<<nt, kPrepThreads, 0, stream>>>(
                 off, ind, deg, n, nnz, trow, tile, foff, find, status);
         }
         const int small_cap = 4 * cfg.group;   // <= kRowSlots / 8
-        vinfo_kernel<<<vb, 256, 0, stream>>>(foff, deg, n, small_cap, cfg.big_chunk, vinfo, big);
+        vinfo_kernel<<<vb, 256, 0, stream>>>(foff, deg, rank_labels ? rank : nullptr, n, small_cap,
+                                             cfg.big_chunk, vinfo, big);
         err = exclusive_scan_i64(big, big, n, scan_tmp, stream);
         if (err != cudaSuccess) return GTC_ERR_CUDA;
         if (timing) cudaEventRecord(timing->ev[1], stream);
+        const int *lorder = rank_labels ? order : nullptr;
         if (nnz > 0) {
             const long long n_items = div_up<long long>(nnz, cfg.item_len);
             item_rows_kernel<OffT><<<(unsigned)div_up<long long>(n_items, 256), 256, 0, stream>>>(
@@ -1063,23 +1457,28 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                 if (need < blocks) blocks = (int)need;
                 kern<<<blocks, kRowThreads, 0, stream>>>(off, ind, n, nnz, vinfo, find, tacc, ctr,
                                                          status, irow, n_items, cfg.item_len,
-                                                         small_cap);
+                                                         small_cap, lorder);
             };
             if (per_vertex) launch_rows(count_rows_kernel<true, OffT>);
             else launch_rows(count_rows_kernel<false, OffT>);
             if (timing) cudaEventRecord(timing->ev[2], stream);
             const size_t big_smem = sizeof(int) * kBigTableSlots +
                                     sizeof(unsigned int) * (kBigTableSlots / 2);
-            auto launch_big = [&](auto kern) {
+            auto launch_big = [&](auto kern, int *cache) {
                 cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem);
-                int blocks = occupancy_blocks(kern, kBigThreads, big_smem, dev,
-                                              &g_big_blocks[dev & 63][per_vertex ? 1 : 0]);
+                int blocks = occupancy_blocks(kern, kBigThreads, big_smem, dev, cache);
                 kern<<<blocks, kBigThreads, big_smem, stream>>>(off, ind, n, vinfo, find, tacc, ctr,
                                                                 status, big, cfg.big_chunk,
-                                                                cfg.big_hash_max);
+                                                                cfg.big_hash_max, lorder);
             };
-            if (per_vertex) launch_big(count_big_kernel<true, OffT>);
-            else launch_big(count_big_kernel<false, OffT>);
+            int *bc = g_big_blocks[dev & 63];
+            if (rank_labels) {
+                if (per_vertex) launch_big(count_big_kernel<true, OffT, true>, &bc[3]);
+                else launch_big(count_big_kernel<false, OffT, true>, &bc[2]);
+            } else {
+                if (per_vertex) launch_big(count_big_kernel<true, OffT, false>, &bc[1]);
+                else launch_big(count_big_kernel<false, OffT, false>, &bc[0]);
+            }
         } else if (timing) {
             cudaEventRecord(timing->ev[2], stream);
         }

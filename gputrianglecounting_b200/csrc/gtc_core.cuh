@@ -13,7 +13,16 @@ struct RowConfig {
     int big_chunk = 2048; // adjacency entries per block-kernel item
     int big_hash_max = kBigHashMaxFdeg;  // longest list hashed by the block kernel
     bool prep_gather = true;  // forward build: gather all degrees first (skewed graphs)
+    bool rank_labels = true;  // label vertices by degree rank (skewed graphs); implies prep_gather
 };
+
+// Kernel launches of one run_count with this configuration (the epilogue
+// kernels counted as launched).
+int launches_per_count(const RowConfig &cfg, bool per_vertex);
+
+// Apply caller overrides (gtc_tuning, 0 = keep) to cfg; GTC_ERR_INVALID_ARGUMENT
+// for a value outside the documented ranges.
+gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning);
 
 // Optional CUDA events recorded between the pipeline phases:
 // ev[0] start, ev[1] forward lists built, ev[2] group kernel done,

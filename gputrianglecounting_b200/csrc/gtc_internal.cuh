@@ -42,6 +42,19 @@ constexpr int kBigHashMaxFdeg = kBigTableSlots / 4;   // load factor <= 1/4
 
 constexpr int kScanThreads = 1024;
 
+// Degree-rank labels (skewed graphs): vertices are ordered by degree (a
+// counting sort over kRankBuckets degree buckets; degrees above the last
+// bucket share it) and every forward list holds the ranks of its members,
+// sorted ascending.
+constexpr int kRankBuckets = 1 << 13;
+constexpr int kRankScanThreads = 1024;
+constexpr int kRankThreads = 256;           // histogram / rank kernels
+constexpr int kRankChunk = 4096;            // vertices per histogram / rank block
+constexpr int kSortThreads = 256;           // forward-list sort kernel (warp per 32 rows)
+constexpr int kSortRegMax = 1024;           // longest list sorted in registers
+constexpr int kBitWords = 4096;             // block kernel rank bitmap: 131072 ranks
+constexpr int kBitKeys = 8192;              // longest apex list on the bitmap path
+
 // Error bits written to the workspace status word by device code.
 enum : unsigned int {
     kErrIndexRange = 1u,   // a neighbour id outside [0, n) was met
@@ -49,17 +62,21 @@ enum : unsigned int {
 };
 
 // Per-vertex record built once per count: forward-list start, forward degree
-// and full degree in one 16-byte load.
+// and the vertex's order key in one 16-byte load.  The key is the degree
+// (vertex-id labels: order by (degree, id)) or the degree rank (rank labels:
+// every key distinct).
 struct __align__(16) VInfo {
     long long fbeg;
     int fdeg;
-    int deg;
+    int key;
 };
 
-// Degree-order rank comparison: does x rank above y?
-__device__ __forceinline__ bool rank_above(int dx, int x, int dy, int y)
+// Order comparison: does x (key kx) come after y (key ky)?  Lexicographic in
+// (key, id), which is the (degree, id) order for degree keys and the rank
+// order for rank keys (distinct keys never reach the id tie-break).
+__device__ __forceinline__ bool rank_above(int kx, int x, int ky, int y)
 {
-    return dx > dy || (dx == dy && x > y);
+    return kx > ky || (kx == ky && x > y);
 }
 
 __device__ __forceinline__ unsigned int hash_slot(int key, int log2_slots)
@@ -102,7 +119,7 @@ struct Plan {
     // workspace byte offsets
     size_t o_status = 0, o_counters = 0, o_deg = 0, o_tile = 0, o_scan_tmp = 0,
            o_foff = 0, o_vinfo = 0, o_find = 0, o_tacc = 0, o_big = 0,
-           o_bigpre = 0, o_trow = 0, o_irow = 0;
+           o_bigpre = 0, o_trow = 0, o_irow = 0, o_hist = 0, o_rank = 0, o_order = 0;
     size_t bytes = 0;
 };
 

@@ -106,13 +106,30 @@ gtc_status gtc_count(const void *d_off, int off_bits, const int32_t *d_ind,
  *   big_chunk    adjacency entries per block-kernel work item (<= 32768)
  *   big_hash_max longest forward list the block kernel hashes in shared
  *                memory (<= 2048); longer lists are binary-searched in place
+ *   labels       how forward lists name vertices: 1 = vertex ids (order by
+ *                (degree, id)), 2 = degree ranks (vertices counting-sorted
+ *                by degree, lists sorted by rank, block kernel on a rank
+ *                bitmap); the library picks ranks for mean degree > 24
  */
 typedef struct gtc_tuning {
     int group;
     int item_len;
     int big_chunk;
     int big_hash_max;
+    int labels;
 } gtc_tuning;
+
+/* Values of gtc_tuning.labels. */
+enum { GTC_LABELS_AUTO = 0, GTC_LABELS_VERTEX_ID = 1, GTC_LABELS_DEGREE_RANK = 2 };
+
+/*
+ * What gtc_count_tuned would run for this graph size and tuning (NULL = the
+ * library's choice), without touching the device: *launches = kernels of one
+ * count (with every output requested), *labels = GTC_LABELS_VERTEX_ID or
+ * GTC_LABELS_DEGREE_RANK.  No counterpart in the reference (introspection).
+ */
+gtc_status gtc_count_launches(int64_t n, int64_t nnz, gtc_mode mode,
+                              const gtc_tuning *tuning, int *launches, int *labels);
 
 gtc_status gtc_count_tuned(const void *d_off, int off_bits,
                            const int32_t *d_ind, int64_t n, int64_t nnz,

@@ -52,6 +52,19 @@ def test_workspace_size_host_only():
     assert lib.gtc_workspace_size(1 << 32, 10, 64, 0, ctypes.byref(out)) == 6
 
 
+def test_launch_plan_host_only():
+    """Label choice and kernel count per configuration, without a device."""
+    from gputrianglecounting_b200 import api
+    assert api.launch_plan(1 << 20, 12 << 20) == {"launches": 16, "labels": "vertex-id"}
+    assert api.launch_plan(1 << 20, 30 << 20) == {"launches": 19, "labels": "degree-rank"}
+    assert api.launch_plan(1 << 20, 30 << 20, mode="oriented")["launches"] == 18
+    assert api.launch_plan(1000, 1000, tuning={"labels": 2})["labels"] == "degree-rank"
+    assert api.launch_plan(1000, 90000, tuning={"labels": 1}) == {"launches": 16,
+                                                                   "labels": "vertex-id"}
+    with pytest.raises(_lib.GTCError):
+        api.launch_plan(1000, 1000, tuning={"labels": 3})
+
+
 def test_invalid_arguments_rejected_before_any_device_work():
     lib = _lib.load()
     # null offsets / workspace
@@ -67,6 +80,9 @@ def test_invalid_arguments_rejected_before_any_device_work():
     assert lib.gtc_count(fake, 32, fake, 10, 4, 0, None, None, None, None, fake, 16, None) == 3
     # bad tuning
     bad = _lib.Tuning(group=12)
+    assert lib.gtc_count_tuned(fake, 32, fake, 10, 4, 0, None, None, None, None, fake, 1 << 20,
+                               None, ctypes.byref(bad)) == 1
+    bad = _lib.Tuning(labels=5)
     assert lib.gtc_count_tuned(fake, 32, fake, 10, 4, 0, None, None, None, None, fake, 1 << 20,
                                None, ctypes.byref(bad)) == 1
     assert lib.gtc_count_subset(None, 32, None, None, -1, None, None) == 1

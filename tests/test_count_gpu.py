@@ -13,10 +13,13 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-TUNINGS = [None, {"group": 4}, {"group": 8}, {"group": 16}, {"group": 32},
+_SHAPES = [{}, {"group": 4}, {"group": 8}, {"group": 16}, {"group": 32},
            {"group": 8, "item_len": 64, "big_chunk": 128},
            {"group": 4, "big_hash_max": 8},     # block kernel's in-place search path
            {"group": 32, "item_len": 32, "big_chunk": 32, "big_hash_max": 16}]
+# every launch shape with vertex-id labels (1) and degree-rank labels (2),
+# plus the library's own choice
+TUNINGS = [None] + [dict(t, labels=lab) for t in _SHAPES for lab in (1, 2)]
 
 
 def _dev(off, ind, dev, off_dtype=torch.int64):
@@ -80,12 +83,26 @@ def test_dense_graph_block_kernel_paths(cuda):
     ind = np.concatenate([np.delete(np.arange(n, dtype=np.int32), i) for i in range(n)])
     d_off, d_ind = _dev(off, ind, cuda)
     counter = api.TriangleCounter(cuda)
-    for tun in (None, {"big_hash_max": 64}, {"group": 4, "big_chunk": 100}):
+    for tun in (None, {"big_hash_max": 64}, {"group": 4, "big_chunk": 100},
+                {"labels": 1}, {"labels": 2}, {"labels": 2, "group": 4, "big_chunk": 100}):
         res = counter.count(d_off, d_ind, tuning=tun)
         torch.cuda.synchronize()
         assert (res.t.cpu().numpy() == math.comb(n - 1, 2)).all()
         assert res.triangles == math.comb(n, 3)
         assert (res.lcc.cpu().numpy() == 1.0).all()
+
+
+def test_rank_labels_large_range(cuda):
+    """Degree-rank labels on a graph with more than 131072 vertices ranked
+    above some block-kernel apexes, so the block kernel also takes its hash
+    table and in-place search paths with rank keys."""
+    g = G.rgg2d(1 << 20, 14, 7).numpy()
+    r_ref, t_ref, lcc_ref, total = O.per_vertex(g.off, g.ind)
+    counter = api.TriangleCounter(cuda)
+    d_off, d_ind = _dev(g.off, g.ind, cuda)
+    for tun in ({"labels": 2, "group": 4}, {"labels": 2, "group": 4, "big_hash_max": 8},
+                {"labels": 2, "group": 4, "big_chunk": 32}):
+        _check(g.off, g.ind, counter.count(d_off, d_ind, tuning=tun), r_ref)
 
 
 def test_edge_cases(cuda):
