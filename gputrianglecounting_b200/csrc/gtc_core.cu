@@ -556,9 +556,12 @@ __device__ void warp_sort_global(int *list, int len, int lane)
     }
 }
 
-// Sort every forward list ascending (rank labels).  One warp per 32
-// consecutive rows, one list at a time: up to kSortRegMax elements in
-// registers, longer lists in place.
+// Sort every forward list longer than kSortMinLen ascending (rank labels).
+// Shorter lists are only ever read whole (as warp-kernel apexes, whose
+// tables do not care about order, or as short partners, whose members are
+// each checked against the apex rank), so they keep id order.  One warp per
+// 32 consecutive rows, one list at a time: in registers up to kSortRegMax
+// elements, in place beyond.
 __global__ void __launch_bounds__(kSortThreads)
 sort_lists_kernel(const long long *__restrict__ foff, long long n, int *__restrict__ find)
 {
@@ -568,12 +571,13 @@ sort_lists_kernel(const long long *__restrict__ foff, long long n, int *__restri
     const long long v = v0 + lane;
     long long b = 0, e = 0;
     if (v < n) { b = foff[v]; e = foff[v + 1]; }
-    unsigned int todo = __ballot_sync(0xffffffffu, e - b >= 2);
+    const long long ln = e - b;
+    unsigned int todo = __ballot_sync(0xffffffffu, ln > kSortMinLen);
     while (todo) {
         const int src = __ffs(todo) - 1;
         todo &= todo - 1;
         const long long lb = __shfl_sync(0xffffffffu, b, src);
-        const int len = (int)(__shfl_sync(0xffffffffu, e, src) - lb);
+        const int len = (int)__shfl_sync(0xffffffffu, ln, src);
         int *list = find + lb;
         if (len <= 32) warp_sort_regs<1>(list, len, lane);
         else if (len <= 64) warp_sort_regs<2>(list, len, lane);
@@ -676,9 +680,15 @@ __device__ __forceinline__ int sorted_find(const int *__restrict__ list,
 //   * the shorter lists are concatenated and swept G probes at a time, each
 //     lane finding its partner by a shuffle binary search over the work
 //     prefix (co-rank).
-// TRIM (rank labels, lists sorted ascending): an element ranked at or below
-// the apex (key ka) cannot be in N+(a), so it is never looked up, and a long
-// partner is swept from its end down to the first element at or below ka.
+// TRIM (rank labels, lists of more than 16 members sorted ascending): an
+// element ranked at or below the apex (key ka) cannot be in N+(a), so it is
+// never looked up, and a long partner is swept from its end down to the
+// first element at or below ka.  With TRIM the block-kernel apex (fa > cap)
+// owns every edge to a lower-ranked neighbour -- probing only the part of
+// its list ranked above the apex -- and an edge to a higher-ranked x only
+// when x is a warp-kernel row (fx <= cap) with fx <= fa; every other edge
+// keeps the longer-list rule, which is the warp kernel's rule, so each edge
+// has exactly one owner.
 // Partner credits: a long partner's hits are one warp reduction; a short
 // partner's hits are the popcount of each batch's hit ballot over the lanes
 // that batch gives it.
@@ -687,7 +697,7 @@ __device__ __forceinline__ int sorted_find(const int *__restrict__ list,
 // Returns this lane's hit count (the apex credit).
 template <int G, bool PER_VERTEX, bool TRIM, typename Grp, class Lookup, class OnHit>
 __device__ __forceinline__ unsigned int
-probe_stride(const Grp &grp, long long s, long long end, int a, int ka, int fa,
+probe_stride(const Grp &grp, long long s, long long end, int a, int ka, int fa, int cap,
              const int *__restrict__ ind, const VInfo *__restrict__ vinfo,
              const int *__restrict__ find, long long n,
              unsigned long long *__restrict__ tacc, unsigned int *status,
@@ -705,7 +715,8 @@ probe_stride(const Grp &grp, long long s, long long end, int a, int ka, int fa,
             fx = ix.fdeg;
             fbx = ix.fbeg;
             const bool fwd = rank_above(ix.key, x, ka, a);
-            partner = fx > 0 && (fwd ? fx <= fa : fx < fa);
+            if (TRIM) partner = fx > 0 && (!fwd || (fx <= cap && fx <= fa));
+            else partner = fx > 0 && (fwd ? fx <= fa : fx < fa);
         } else {
             atomicOr(status, kErrIndexRange);
         }
@@ -1077,11 +1088,12 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
 // binary-searched in global memory.
 // Rank labels: N+(a) lies in the ranks above the apex, (ka, n), so when that
 // range has at most 32*kBitWords ranks the block marks the apex's list in a
-// shared bitmap over it -- one load and one bit test per probe, no
-// collisions -- and keeps per 32-bit word the number of marked ranks below it
-// (pre), so a hit at rank w has index pre + popcount(lower bits of its word)
-// in the sorted apex list, which indexes its 16-bit hit counter.  Larger
-// ranges use the hash table or the binary search, with the rank keys.
+// shared bitmap over it -- one 8-byte load and one bit test per probe, no
+// collisions.  Each 32-bit word of marks travels with the number of marks
+// below it, so a hit at rank w has index (marks below its word) +
+// popcount(lower bits of its word) in the sorted apex list, which indexes
+// its 32-bit hit counter.  Larger ranges use the hash table or the binary
+// search, with the rank keys.
 // Within an item the warps take 32-entry strides from a shared counter, so
 // uneven partner work does not idle the block at its barriers.
 template <bool PER_VERTEX, typename OffT, bool RANK>
@@ -1091,7 +1103,8 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                  const int *__restrict__ find,
                  unsigned long long *__restrict__ tacc, Counters *ctr,
                  unsigned int *status, const long long *__restrict__ big_pre,
-                 int big_chunk, int big_hash_max, const int *__restrict__ order)
+                 int big_chunk, int big_hash_max, int small_cap,
+                 const int *__restrict__ order)
 {
     extern __shared__ int smem[];
     int *keys = smem;
@@ -1131,16 +1144,17 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
         };
         const long long range = RANK ? n - 1 - (long long)ka : 0;
         if (RANK && range <= 32ll * kBitWords && fa <= kBitKeys) {
-            unsigned int *bits = reinterpret_cast<unsigned int *>(smem);
-            unsigned short *pre = reinterpret_cast<unsigned short *>(bits + kBitWords);
+            // word wd: .x = marks of ranks ka+1+32wd .. ka+32+32wd, .y = marks below
+            uint2 *bw = reinterpret_cast<uint2 *>(smem);
+            unsigned int *hitc = hitw;               // one 32-bit counter per apex element
             const int words = (int)((range + 31) >> 5);
-            for (int k = threadIdx.x; k < words; k += kBigThreads) bits[k] = 0;
+            for (int k = threadIdx.x; k < words; k += kBigThreads) bw[k] = make_uint2(0u, 0u);
             if (PER_VERTEX)
-                for (int k = threadIdx.x; k < ((fa + 1) >> 1); k += kBigThreads) hitw[k] = 0;
+                for (int k = threadIdx.x; k < fa; k += kBigThreads) hitc[k] = 0;
             __syncthreads();
             for (int k = threadIdx.x; k < fa; k += kBigThreads) {
                 const unsigned int p = (unsigned int)(alist[k] - ka - 1);
-                atomicOr(&bits[p >> 5], 1u << (p & 31u));
+                atomicOr(&bw[p >> 5].x, 1u << (p & 31u));
             }
             __syncthreads();
             if (PER_VERTEX) {
@@ -1148,7 +1162,7 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                 const int w0 = threadIdx.x * kPer;
                 unsigned int c = 0;
 #pragma unroll
-                for (int k = 0; k < kPer; ++k) c += (w0 + k < words) ? __popc(bits[w0 + k]) : 0u;
+                for (int k = 0; k < kPer; ++k) c += (w0 + k < words) ? __popc(bw[w0 + k].x) : 0u;
                 unsigned int incl = c;
 #pragma unroll
                 for (int d = 1; d < 32; d <<= 1) {
@@ -1162,29 +1176,28 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
 #pragma unroll
                 for (int k = 0; k < kPer; ++k) {
                     if (w0 + k < words) {
-                        pre[w0 + k] = (unsigned short)run;
-                        run += __popc(bits[w0 + k]);
+                        bw[w0 + k].y = run;
+                        run += __popc(bw[w0 + k].x);
                     }
                 }
                 __syncthreads();
             }
-            auto lookup = [bits, pre, ka](int w) -> int {
+            auto lookup = [bw, ka](int w) -> int {
                 const unsigned int p = (unsigned int)(w - ka - 1);
-                const unsigned int word = bits[p >> 5];
+                const uint2 wd = bw[p >> 5];
                 const unsigned int b = p & 31u;
-                if (!((word >> b) & 1u)) return -1;
-                return PER_VERTEX ? (int)pre[p >> 5] + __popc(word & ((1u << b) - 1u)) : 0;
+                if (!((wd.x >> b) & 1u)) return -1;
+                return PER_VERTEX ? (int)(wd.y + __popc(wd.x & ((1u << b) - 1u))) : 0;
             };
-            auto on_hit = [hitw](int slot, int) {
-                atomicAdd(&hitw[slot >> 1], 1u << ((slot & 1) << 4));
-            };
+            auto on_hit = [hitc](int slot, int) { atomicAdd(&hitc[slot], 1u); };
             for (long long s = next_stride(); s < re; s = next_stride())
-                cnt += probe_stride<32, PER_VERTEX, true>(warp, s, re, (int)a, ka, fa, ind, vinfo,
-                                                          find, n, tacc, status, lookup, on_hit);
+                cnt += probe_stride<32, PER_VERTEX, true>(warp, s, re, (int)a, ka, fa, small_cap,
+                                                          ind, vinfo, find, n, tacc, status,
+                                                          lookup, on_hit);
             __syncthreads();
             if (PER_VERTEX) {
                 for (int k = threadIdx.x; k < fa; k += kBigThreads) {
-                    const unsigned int c = (hitw[k >> 1] >> ((k & 1) << 4)) & 0xffffu;
+                    const unsigned int c = hitc[k];
                     if (c) atomicAdd(&tacc[order[alist[k]]], (unsigned long long)c);
                 }
             }
@@ -1201,8 +1214,9 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
             auto lookup = [tab](int w) { return tab.find(w); };
             auto on_hit = [tab](int slot, int) { tab.add_hit(slot); };
             for (long long s = next_stride(); s < re; s = next_stride())
-                cnt += probe_stride<32, PER_VERTEX, RANK>(warp, s, re, (int)a, ka, fa, ind, vinfo,
-                                                          find, n, tacc, status, lookup, on_hit);
+                cnt += probe_stride<32, PER_VERTEX, RANK>(warp, s, re, (int)a, ka, fa, small_cap,
+                                                          ind, vinfo, find, n, tacc, status,
+                                                          lookup, on_hit);
             __syncthreads();
             if (PER_VERTEX) flush_hits(tab, tsize, threadIdx.x, kBigThreads, tacc, order);
         } else {
@@ -1211,8 +1225,9 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                 atomicAdd(&tacc[label_vertex(order, w)], 1ull);
             };
             for (long long s = next_stride(); s < re; s = next_stride())
-                cnt += probe_stride<32, PER_VERTEX, RANK>(warp, s, re, (int)a, ka, fa, ind, vinfo,
-                                                          find, n, tacc, status, lookup, on_hit);
+                cnt += probe_stride<32, PER_VERTEX, RANK>(warp, s, re, (int)a, ka, fa, small_cap,
+                                                          ind, vinfo, find, n, tacc, status,
+                                                          lookup, on_hit);
         }
         const unsigned int wsum = cg::reduce(warp, cnt, cg::plus<unsigned int>());
         if (lane == 0 && wsum) atomicAdd(&s_cnt, wsum);
@@ -1469,7 +1484,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                 int blocks = occupancy_blocks(kern, kBigThreads, big_smem, dev, cache);
                 kern<<<blocks, kBigThreads, big_smem, stream>>>(off, ind, n, vinfo, find, tacc, ctr,
                                                                 status, big, cfg.big_chunk,
-                                                                cfg.big_hash_max, lorder);
+                                                                cfg.big_hash_max, small_cap, lorder);
             };
             int *bc = g_big_blocks[dev & 63];
             if (rank_labels) {

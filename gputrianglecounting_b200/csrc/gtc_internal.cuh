@@ -53,7 +53,9 @@ constexpr int kRankChunk = 4096;            // vertices per histogram / rank blo
 constexpr int kSortThreads = 256;           // forward-list sort kernel (warp per 32 rows)
 constexpr int kSortRegMax = 1024;           // longest list sorted in registers
 constexpr int kBitWords = 4096;             // block kernel rank bitmap: 131072 ranks
-constexpr int kBitKeys = 8192;              // longest apex list on the bitmap path
+constexpr int kBitKeys = 4096;              // longest apex list on the bitmap path
+constexpr int kSortMinLen = 16;             // lists up to this long are left unsorted
+                                            // (the smallest block-kernel cap is 4 * 4)
 
 // Error bits written to the workspace status word by device code.
 enum : unsigned int {
