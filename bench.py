@@ -392,11 +392,11 @@ def run_b200(args, cfg, rank: int, world: int):
     return line
 
 
-def launches_per_count(n: int, nnz: int) -> int:
+def launches_per_count(n: int, nnz: int, tuning: dict | None = None) -> int:
     """Kernels of one plain count with every output (the library's own plan:
     16 with vertex-id labels, 19 with degree-rank labels)."""
     from gputrianglecounting_b200 import api
-    return api.launch_plan(n, nnz)["launches"]
+    return api.launch_plan(n, nnz, tuning=tuning)["launches"]
 
 
 def phase_breakdown(counter, g, flush) -> dict:
@@ -426,10 +426,10 @@ def phase_breakdown(counter, g, flush) -> dict:
 
 # ------------------------------------------------------------------ batched
 
-def batch_launches(total_n: int, total_nnz: int) -> int:
+def batch_launches(total_n: int, total_nnz: int, tuning: dict | None = None) -> int:
     """Entry starts + globalize + the pipeline without its global-count
     kernel + per-graph T."""
-    return 2 + (launches_per_count(total_n, total_nnz) - 1) + 1
+    return 2 + (launches_per_count(total_n, total_nnz, tuning) - 1) + 1
 
 
 def run_batched(args, cfg, rank: int, world: int):
@@ -453,14 +453,21 @@ def run_batched(args, cfg, rank: int, world: int):
     m_total = batch.total_nnz // 2
     bc = api.BatchCounter(dev)
     out = bc.alloc_outputs(batch, ("r", "lcc", "graph_T"))
+    # tuning for this batch's degree profile (staged search, cached), chosen
+    # before any timed step
+    from gputrianglecounting_b200 import autotune
+    t0 = time.perf_counter()
+    tuning = autotune.autotune_batch(bc, batch, out=out)
+    tune_s = time.perf_counter() - t0
+    tune_entry = autotune.batch_entry(batch)
     stream = torch.cuda.Stream(dev)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
-            bc.count(batch, out=out, stream=stream)
+            bc.count(batch, out=out, tuning=tuning, stream=stream)
     stream.synchronize()
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph, stream=stream):
-        bc.count(batch, out=out, stream=stream)
+        bc.count(batch, out=out, tuning=tuning, stream=stream)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
     if world > 1:
@@ -514,11 +521,13 @@ def run_batched(args, cfg, rank: int, world: int):
                    "l2": "inputs (13 GB adjacency) far larger than L2",
                    "generation_s": gen_s, "parallelism": f"{world} independent replica(s)"},
         "batched": {"form": "one gtc_count_batch per step, captured CUDA graph, persistent kernels",
+                    "tuning": tuning, "tuning_search_s": tune_s,
+                    "untuned_step_ms": tune_entry["default_ms"] if tune_entry else None,
                     "edges_per_s": value, "step_ms_p50": p(0.5), "step_ms_p99": p(0.99),
                     "per_graph_ms": min(base_ms), "per_graph_edges_per_s": base_value,
                     "speedup_vs_one_call_per_graph": value / world / base_value},
         "clocks": clk.result,
-        "gpu_launches": batch_launches(batch.total_n, batch.total_nnz) * args.steps,
+        "gpu_launches": batch_launches(batch.total_n, batch.total_nnz, tuning) * args.steps,
     }
     if not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -554,7 +563,11 @@ def run_serving(args, cfg, rank: int, world: int):
     big = [G.rmat(22, 16, cfg["seed"] * 10 + k, device=dev) for k in range(2)]
     graphs = pool + big
     torch.cuda.synchronize()
-    server = serve.CountServer(graphs, dev, slots=3, budget_bytes=4 << 30, max_graphs=512)
+    # launch shape tuned once on the pool's union (the typical admitted batch)
+    from gputrianglecounting_b200 import api, autotune
+    tuning = autotune.autotune_batch(api.BatchCounter(dev), G.concat_graphs(pool, dev))
+    server = serve.CountServer(graphs, dev, slots=3, budget_bytes=4 << 30, max_graphs=512,
+                               tuning=tuning)
     # warm-up: every graph once, to size the slots' workspaces
     warm = [serve.Request(i, i, 0.0) for i in range(len(graphs))]
     server.run(warm)
@@ -584,7 +597,7 @@ def run_serving(args, cfg, rank: int, world: int):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32 ids / int64 counts", "data": "synthetic",
         "config": {"workload": "serving", "graph": cfg["label"], "slots": 3,
-                   "slot_budget_gb": 4, "max_graphs_per_batch": 512},
+                   "slot_budget_gb": 4, "max_graphs_per_batch": 512, "tuning": tuning},
         "serving": per_rate, "clocks": clk.result,
     }
     return line

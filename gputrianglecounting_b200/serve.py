@@ -99,9 +99,10 @@ class _Slot:
 class CountServer:
     def __init__(self, graphs, device=None, slots: int = 3, budget_bytes: int = 6 << 30,
                  max_graphs: int = 512, keep_vertex_results: bool = False,
-                 large_nnz: int = 16 << 20):
+                 large_nnz: int = 16 << 20, tuning: dict | None = None):
         """graphs: device-resident CSRGraphs (int64 off, int32 ind) that
-        requests refer to by index."""
+        requests refer to by index; tuning: launch shape for every batch
+        (e.g. from autotune.autotune_batch), None = the library's choice."""
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
         self.graphs = graphs
@@ -113,6 +114,7 @@ class CountServer:
         self.queue: deque[Request] = deque()          # small requests
         self.large: deque[Request] = deque()          # large requests
         self.large_nnz = large_nnz
+        self.tuning = tuning
         self.batches = 0
 
     # ---- slots
@@ -121,7 +123,7 @@ class CountServer:
         with torch.cuda.stream(slot.stream):
             batch = slot.counter.pack(gs, stream=slot.stream)
             out = slot.counter.count(batch, outputs=("r", "graph_T") if self.keep else ("graph_T",),
-                                     stream=slot.stream)
+                                     stream=slot.stream, tuning=self.tuning)
             ev = torch.cuda.Event()
             ev.record(slot.stream)
         slot.event, slot.requests, slot.out, slot.batch = ev, reqs, out, batch
