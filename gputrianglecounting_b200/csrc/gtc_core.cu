@@ -655,7 +655,7 @@ struct ApexTable {
 // Lanes [lo, hi) of a batch as a bit mask (0 <= lo < hi <= 32).
 __device__ __forceinline__ unsigned int lane_range(int lo, int hi)
 {
-    return (unsigned int)(((1ull << hi) - 1ull) & ~((1ull << lo) - 1ull));
+    return (0xffffffffu >> (32 - hi)) & (0xffffffffu << lo);
 }
 
 // Binary search of a sorted global forward list (block kernel, apexes whose
@@ -962,6 +962,7 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
             const int ts = act ? (1 << lg) : 0;
             const int tincl = warp_incl_scan(ts);
             const int toff = tincl - ts;
+            const int rdesc = toff | (lg << 16);      // region: offset | log2(size) << 16
             const bool take = in_item && tincl <= kRowSlots;
             const unsigned int tmask = __ballot_sync(0xffffffffu, take);
             const int nrows = __popc(tmask);          // a prefix of the lanes
@@ -981,11 +982,9 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                 for (int f0 = 0; f0 < ftot; f0 += 32) {
                     const int f = f0 + lane;
                     const int i = warp_corank(fincl, f);
-                    const long long fb_i = __shfl_sync(0xffffffffu, vi.fbeg, i);
-                    const int ex_i = __shfl_sync(0xffffffffu, fexcl, i);
-                    const int to_i = __shfl_sync(0xffffffffu, toff, i);
-                    const int lg_i = __shfl_sync(0xffffffffu, lg, i);
-                    if (f < ftot) region_insert(keys, to_i, lg_i, find[fb_i + (f - ex_i)]);
+                    const long long fb_i = __shfl_sync(0xffffffffu, vi.fbeg - fexcl, i);
+                    const int rd_i = __shfl_sync(0xffffffffu, rdesc, i);
+                    if (f < ftot) region_insert(keys, rd_i & 0xffff, rd_i >> 16, find[fb_i + f]);
                 }
                 __syncwarp();
                 // ---- 3. scan the active rows' entries for partners, probe
@@ -996,18 +995,16 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                 for (int c0 = 0; c0 < ltot; c0 += 32) {
                     const int f = c0 + lane;
                     const int i = warp_corank(lincl, f);
-                    const long long s0_i = __shfl_sync(0xffffffffu, s0, i);
-                    const int ex_i = __shfl_sync(0xffffffffu, lexcl, i);
+                    const long long s0_i = __shfl_sync(0xffffffffu, s0 - lexcl, i);
                     const int fa_i = __shfl_sync(0xffffffffu, vi.fdeg, i);
                     const int ka_i = __shfl_sync(0xffffffffu, vi.key, i);
-                    const int to_i = __shfl_sync(0xffffffffu, toff, i);
-                    const int lg_i = __shfl_sync(0xffffffffu, lg, i);
+                    const int rd_i = __shfl_sync(0xffffffffu, rdesc, i);
                     const int a = (int)(ra + i);
                     bool partner = false;
                     int x = 0, fx = 0;
                     long long fbx = 0;
                     if (f < ltot) {
-                        x = ind[s0_i + (f - ex_i)];
+                        x = ind[s0_i + f];
                         if ((unsigned long long)(long long)x < (unsigned long long)n) {
                             const VInfo ix = vinfo[x];
                             fx = ix.fdeg;
@@ -1023,16 +1020,15 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                     const int ptot = __shfl_sync(0xffffffffu, pincl, 31);
                     const int pexcl = pincl - pw;
                     unsigned int mine = 0;
+                    const long long pbase = fbx - pexcl;      // list base minus its probe offset
                     for (int g0 = 0; g0 < ptot; g0 += 32) {
                         const int g = g0 + lane;
                         const int p = warp_corank(pincl, g);
-                        const long long fb_p = __shfl_sync(0xffffffffu, fbx, p);
-                        const int ex_p = __shfl_sync(0xffffffffu, pexcl, p);
-                        const int to_p = __shfl_sync(0xffffffffu, to_i, p);
-                        const int lg_p = __shfl_sync(0xffffffffu, lg_i, p);
+                        const long long fb_p = __shfl_sync(0xffffffffu, pbase, p);
+                        const int rd_p = __shfl_sync(0xffffffffu, rd_i, p);
                         bool hit = false;
                         if (g < ptot) {
-                            const int slot = region_find(keys, to_p, lg_p, find[fb_p + (g - ex_p)]);
+                            const int slot = region_find(keys, rd_p & 0xffff, rd_p >> 16, find[fb_p + g]);
                             if (slot >= 0) {
                                 hit = true;
                                 if (PER_VERTEX) atomicAdd(&hitw[slot >> 1], 1u << ((slot & 1) << 4));
@@ -1044,13 +1040,16 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                             if (lo < hi) mine += __popc(hm & lane_range(lo, hi));
                         }
                     }
-                    if (mine) {
-                        if (PER_VERTEX) {
-                            atomicAdd(&tacc[x], (unsigned long long)mine);
-                            atomicAdd(&tacc[a], (unsigned long long)mine);
-                        }
-                        tri_local += mine;
+                    // partner credits per lane; apex credits summed over the
+                    // lanes of each row first (one atomic per row and chunk)
+                    if (PER_VERTEX) {
+                        if (mine) atomicAdd(&tacc[x], (unsigned long long)mine);
+                        const unsigned int same = __match_any_sync(0xffffffffu, i);
+                        const unsigned int rsum = __reduce_add_sync(same, mine);
+                        if (rsum && lane == __ffs(same) - 1)
+                            atomicAdd(&tacc[a], (unsigned long long)rsum);
                     }
+                    tri_local += mine;
                 }
                 __syncwarp();
                 // ---- 4. third-vertex credits
