@@ -561,32 +561,38 @@ __device__ void warp_sort_global(int *list, int len, int lane)
 // tables do not care about order, or as short partners, whose members are
 // each checked against the apex rank), so they keep id order.  One warp per
 // 32 consecutive rows, one list at a time: in registers up to kSortRegMax
-// elements, in place beyond.
+// elements, in place beyond.  Groups come from a dynamic queue, so the few
+// groups holding several long lists do not set the kernel's length.
 __global__ void __launch_bounds__(kSortThreads)
-sort_lists_kernel(const long long *__restrict__ foff, long long n, int *__restrict__ find)
+sort_lists_kernel(const long long *__restrict__ foff, long long n, int *__restrict__ find,
+                  Counters *ctr)
 {
     const int lane = threadIdx.x & 31;
-    const long long v0 = ((long long)blockIdx.x * (kSortThreads / 32) + (threadIdx.x >> 5)) * 32;
-    if (v0 >= n) return;
-    const long long v = v0 + lane;
-    long long b = 0, e = 0;
-    if (v < n) { b = foff[v]; e = foff[v + 1]; }
-    const long long ln = e - b;
-    unsigned int todo = __ballot_sync(0xffffffffu, ln > kSortMinLen);
-    while (todo) {
-        const int src = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const long long lb = __shfl_sync(0xffffffffu, b, src);
-        const int len = (int)__shfl_sync(0xffffffffu, ln, src);
-        int *list = find + lb;
-        if (len <= 32) warp_sort_regs<1>(list, len, lane);
-        else if (len <= 64) warp_sort_regs<2>(list, len, lane);
-        else if (len <= 128) warp_sort_regs<4>(list, len, lane);
-        else if (len <= 256) warp_sort_regs<8>(list, len, lane);
-        else if (len <= 512) warp_sort_regs<16>(list, len, lane);
-        else if (len <= kSortRegMax) warp_sort_regs<32>(list, len, lane);
-        else warp_sort_global(list, len, lane);
-        __syncwarp();
+    while (true) {
+        unsigned long long grp = 0;
+        if (lane == 0) grp = atomicAdd(&ctr->sort_groups, 1ull);
+        const long long v0 = (long long)__shfl_sync(0xffffffffu, grp, 0) * 32;
+        if (v0 >= n) break;
+        const long long v = v0 + lane;
+        long long b = 0, e = 0;
+        if (v < n) { b = foff[v]; e = foff[v + 1]; }
+        const long long ln = e - b;
+        unsigned int todo = __ballot_sync(0xffffffffu, ln > kSortMinLen);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const long long lb = __shfl_sync(0xffffffffu, b, src);
+            const int len = (int)__shfl_sync(0xffffffffu, ln, src);
+            int *list = find + lb;
+            if (len <= 32) warp_sort_regs<1>(list, len, lane);
+            else if (len <= 64) warp_sort_regs<2>(list, len, lane);
+            else if (len <= 128) warp_sort_regs<4>(list, len, lane);
+            else if (len <= 256) warp_sort_regs<8>(list, len, lane);
+            else if (len <= 512) warp_sort_regs<16>(list, len, lane);
+            else if (len <= kSortRegMax) warp_sort_regs<32>(list, len, lane);
+            else warp_sort_global(list, len, lane);
+            __syncwarp();
+        }
     }
 }
 
@@ -1085,10 +1091,12 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
 // kBigTableSlots slots (load factor <= 1/8 up to kBigTableSlots/8 keys,
 // <= 1/4 up to kBigHashMaxFdeg); beyond big_hash_max the apex list is
 // binary-searched in global memory.
-// Rank labels: N+(a) lies in the ranks above the apex, (ka, n), so when that
-// range has at most 32*kBitWords ranks the block marks the apex's list in a
-// shared bitmap over it -- one 8-byte load and one bit test per probe, no
-// collisions.  Each 32-bit word of marks travels with the number of marks
+// Rank labels: N+(a) lies in the ranks above the apex, (ka, n).  When that
+// range has at most kDirectRanks ranks, the block keeps one 16-bit counter
+// per rank in it (0xffff for ranks outside N+(a)): a probe is one 2-byte
+// load and a compare, a hit one packed shared atomic.  Up to 32*kBitWords
+// ranks, the block marks the apex's list in a shared bitmap over the range
+// -- one 8-byte load and one bit test per probe, no collisions.  Each 32-bit word of marks travels with the number of marks
 // below it, so a hit at rank w has index (marks below its word) +
 // popcount(lower bits of its word) in the sorted apex list, which indexes
 // its 32-bit hit counter.  Larger ranges use the hash table or the binary
@@ -1142,7 +1150,36 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
             return rb + 32ll * warp.shfl(st, 0);
         };
         const long long range = RANK ? n - 1 - (long long)ka : 0;
-        if (RANK && range <= 32ll * kBitWords && fa <= kBitKeys) {
+        if (RANK && range <= kDirectRanks) {
+            // one 16-bit counter per rank above the apex; 0xffff marks a
+            // rank outside N+(a), so the counter is also the membership test
+            unsigned short *cnt16 = reinterpret_cast<unsigned short *>(smem);
+            unsigned int *cnt32 = reinterpret_cast<unsigned int *>(smem);
+            const int words = (int)((range + 1) >> 1);
+            for (int k = threadIdx.x; k < words; k += kBigThreads) cnt32[k] = 0xffffffffu;
+            __syncthreads();
+            for (int k = threadIdx.x; k < fa; k += kBigThreads) cnt16[alist[k] - ka - 1] = 0;
+            __syncthreads();
+            auto lookup = [cnt16, ka](int w) -> int {
+                const int p = w - ka - 1;
+                return cnt16[p] != 0xffffu ? p : -1;
+            };
+            auto on_hit = [cnt32](int p, int) {
+                atomicAdd(&cnt32[p >> 1], 1u << ((p & 1) << 4));
+            };
+            for (long long s = next_stride(); s < re; s = next_stride())
+                cnt += probe_stride<32, PER_VERTEX, true>(warp, s, re, (int)a, ka, fa, small_cap,
+                                                          ind, vinfo, find, n, tacc, status,
+                                                          lookup, on_hit);
+            __syncthreads();
+            if (PER_VERTEX) {
+                for (int k = threadIdx.x; k < fa; k += kBigThreads) {
+                    const int w = alist[k];
+                    const unsigned int c = cnt16[w - ka - 1];
+                    if (c) atomicAdd(&tacc[order[w]], (unsigned long long)c);
+                }
+            }
+        } else if (RANK && range <= 32ll * kBitWords && fa <= kBitKeys) {
             // word wd: .x = marks of ranks ka+1+32wd .. ka+32+32wd, .y = marks below
             uint2 *bw = reinterpret_cast<uint2 *>(smem);
             unsigned int *hitc = hitw;               // one 32-bit counter per apex element
@@ -1277,6 +1314,7 @@ namespace {
 int g_sm_count[64];
 int g_rows_blocks[64][8];
 int g_big_blocks[64][4];
+int g_sort_blocks[64];
 
 int device_sm_count(int dev)
 {
@@ -1444,8 +1482,11 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
         if (rank_labels) {
             tile_fill_kernel<OffT, true><<<nt, kPrepThreads, 0, stream>>>(
                 off, ind, rank, n, nnz, trow, tile, foff, find, status);
-            sort_lists_kernel<<<(unsigned)div_up<long long>(n, 32 * (kSortThreads / 32)),
-                                kSortThreads, 0, stream>>>(foff, n, find);
+            long long sb = occupancy_blocks(sort_lists_kernel, kSortThreads, 0, dev,
+                                            &g_sort_blocks[dev & 63]);
+            const long long sneed = div_up<long long>(n, 32 * (kSortThreads / 32));
+            if (sneed < sb) sb = sneed;
+            sort_lists_kernel<<<(unsigned)sb, kSortThreads, 0, stream>>>(foff, n, find, ctr);
         } else if (cfg.prep_gather) {
             tile_fill_kernel<OffT, false><<<nt, kPrepThreads, 0, stream>>>(
                 off, ind, deg, n, nnz, trow, tile, foff, find, status);

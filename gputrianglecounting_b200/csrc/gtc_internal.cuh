@@ -52,6 +52,7 @@ constexpr int kRankThreads = 256;           // histogram / rank kernels
 constexpr int kRankChunk = 4096;            // vertices per histogram / rank block
 constexpr int kSortThreads = 256;           // forward-list sort kernel (warp per 32 rows)
 constexpr int kSortRegMax = 1024;           // longest list sorted in registers
+constexpr int kDirectRanks = 24576;         // block kernel: one 16-bit counter per rank
 constexpr int kBitWords = 4096;             // block kernel rank bitmap: 131072 ranks
 constexpr int kBitKeys = 4096;              // longest apex list on the bitmap path
 constexpr int kSortMinLen = 16;             // lists up to this long are left unsorted
@@ -131,7 +132,8 @@ struct Counters {
     unsigned long long row_items;     // dynamic item queue, group kernel
     unsigned long long big_items;     // dynamic item queue, block kernel
     unsigned long long big_rows;      // number of rows for the block kernel
-    unsigned long long pad[4];
+    unsigned long long sort_groups;   // dynamic queue of 32-row groups, list sort
+    unsigned long long pad[3];
 };
 
 size_t scan_tmp_bytes(long long count);
