@@ -739,23 +739,26 @@ probe_stride(const Grp &grp, long long s, long long end, int a, int ka, int fa, 
         const int px = grp.shfl(x, src);
         unsigned int hx = 0;
         if (TRIM) {
-            for (int top = len; top > 0; top -= 2 * G) {
-                const int j0 = top - G + lane, j1 = top - 2 * G + lane;
-                const int w0 = j0 >= 0 ? list[j0] : ka;
-                const int w1 = j1 >= 0 ? list[j1] : ka;
-                const int s0 = w0 > ka ? lookup(w0) : -1;
-                const int s1 = w1 > ka ? lookup(w1) : -1;
-                if (s0 >= 0) {
-                    ++hx;
-                    if (PER_VERTEX) on_hit(s0, w0);
+            // windows of kTrimLoads * G elements from the end, all loads of a
+            // window in flight together
+            for (int top = len; top > 0; top -= kTrimLoads * G) {
+                int w[kTrimLoads];
+#pragma unroll
+                for (int u = 0; u < kTrimLoads; ++u) {
+                    const int j = top - (u + 1) * G + lane;
+                    w[u] = j >= 0 ? list[j] : ka;
                 }
-                if (s1 >= 0) {
-                    ++hx;
-                    if (PER_VERTEX) on_hit(s1, w1);
+#pragma unroll
+                for (int u = 0; u < kTrimLoads; ++u) {
+                    const int sl = w[u] > ka ? lookup(w[u]) : -1;
+                    if (sl >= 0) {
+                        ++hx;
+                        if (PER_VERTEX) on_hit(sl, w[u]);
+                    }
                 }
                 // sorted: once a loaded element is at or below ka, so is
                 // every element before it (lanes past the list start load ka)
-                if (grp.any(w1 <= ka)) break;
+                if (grp.any(w[kTrimLoads - 1] <= ka)) break;
             }
         } else {
             int j = lane;

@@ -53,6 +53,7 @@ constexpr int kRankChunk = 4096;            // vertices per histogram / rank blo
 constexpr int kSortThreads = 256;           // forward-list sort kernel (warp per 32 rows)
 constexpr int kSortRegMax = 1024;           // longest list sorted in registers
 constexpr int kDirectRanks = 24576;         // block kernel: one 16-bit counter per rank
+constexpr int kTrimLoads = 4;               // block kernel: loads in flight per partner window
 constexpr int kBitWords = 4096;             // block kernel rank bitmap: 131072 ranks
 constexpr int kBitKeys = 4096;              // longest apex list on the bitmap path
 constexpr int kSortMinLen = 16;             // lists up to this long are left unsorted
