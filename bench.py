@@ -56,12 +56,12 @@ CONFIGS = {
 }
 
 
-# DRAM bytes (read + write) of one complete count, summed over its 16 launches
+# DRAM bytes (read + write) of one complete count, summed over its launches
 # from one ncu capture of this same workload (dram__bytes_read.sum +
 # dram__bytes_write.sum, cold L2 before each launch).  Far below B_alg: the
 # forward lists and the per-vertex records stay in the 126 MB L2, so most
 # probe reads never reach HBM.
-DRAM_TRAFFIC = {"rmat20": 1081080832, "rgg": 1402710528}
+DRAM_TRAFFIC = {"rmat20": 1183645440, "rgg": 1402203904}
 
 
 def make_graph(cfg: dict, device):
