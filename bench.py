@@ -394,7 +394,7 @@ def run_b200(args, cfg, rank: int, world: int):
 
 def launches_per_count(n: int, nnz: int, tuning: dict | None = None) -> int:
     """Kernels of one plain count with every output (the library's own plan:
-    16 with vertex-id labels, 19 with degree-rank labels)."""
+    13 with vertex-id labels, 15 with degree-rank labels)."""
     from gputrianglecounting_b200 import api
     return api.launch_plan(n, nnz, tuning=tuning)["launches"]
 

@@ -180,13 +180,17 @@ struct TileSmem {
 template <typename OffT>
 __global__ void tile_bounds_kernel(const OffT *__restrict__ off, long long n,
                                    long long nnz, long long n_tiles,
-                                   long long *__restrict__ trow)
+                                   long long *__restrict__ trow, int *__restrict__ fcnt)
 {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t > n_tiles) return;
     long long d = t * kPrepTile;
     if (d > n + nnz) d = n + nnz;
-    trow[t] = mp_rows(off, n, nnz, d);
+    const long long r = mp_rows(off, n, nnz, d);
+    trow[t] = r;
+    // the row holding this boundary may be split between two tiles, which
+    // then add their forward counts to fcnt[r]
+    if (r < n) fcnt[r] = 0;
 }
 
 template <typename OffT>
@@ -227,119 +231,6 @@ __device__ __forceinline__ void tile_thread_start(const TileSmem &s,
     }
     li = lo;
     lj = ld - lo;
-}
-
-// Forward flag of the entry at local (li, lj): does ind[e] outrank the row?
-__device__ __forceinline__ bool entry_forward(const TileSmem &s, long long li,
-                                              long long lj,
-                                              const int *__restrict__ deg,
-                                              long long n,
-                                              unsigned int *status)
-{
-    const long long a = s.r0 + li;
-    const int da = (int)(s.off[li + 1] - s.off[li]);
-    const int x = s.ind[lj];
-    if ((unsigned long long)(long long)x >= (unsigned long long)n) {
-        atomicOr(status, kErrIndexRange);
-        return false;
-    }
-    return rank_above(deg[x], x, da, (int)a);
-}
-
-// Pass 1, walking the items in order (one degree gather per entry): for
-// graphs whose neighbours are close in id and in cache, where the smaller
-// register footprint keeps more tiles resident.
-template <typename OffT>
-__global__ void __launch_bounds__(kPrepThreads)
-tile_count_seq_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
-                  const int *__restrict__ deg, long long n, long long nnz,
-                  const long long *__restrict__ trow,
-                  long long *__restrict__ tile_cnt, unsigned int *status)
-{
-    __shared__ TileSmem s;
-    tile_stage(s, off, ind, n, nnz, trow);
-    long long li, lj;
-    tile_thread_start(s, li, lj);
-    const long long rows = s.r1 - s.r0, ents = s.e1 - s.e0;
-    int cnt = 0;
-#pragma unroll
-    for (int k = 0; k < kPrepItemsPerThread; ++k) {
-        if (li + lj >= rows + ents) break;
-        if (li < rows && lj >= s.off[li + 1] - s.e0) {
-            ++li;                                   // row end
-        } else {
-            cnt += entry_forward(s, li, lj, deg, n, status);
-            ++lj;
-        }
-    }
-    __shared__ int warp_sum[kPrepThreads / 32];
-    int w = cnt;
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
-    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = w;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        long long t = 0;
-        for (int i = 0; i < kPrepThreads / 32; ++i) t += warp_sum[i];
-        tile_cnt[blockIdx.x] = t;
-    }
-}
-
-// Pass 2, walking the items in order (see pass 1).
-template <typename OffT>
-__global__ void __launch_bounds__(kPrepThreads)
-tile_fill_seq_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
-                 const int *__restrict__ deg, long long n, long long nnz,
-                 const long long *__restrict__ trow,
-                 const long long *__restrict__ tile_pre,
-                 long long *__restrict__ foff, int *__restrict__ find,
-                 unsigned int *status)
-{
-    __shared__ TileSmem s;
-    __shared__ int warp_sum[kPrepThreads / 32];
-    tile_stage(s, off, ind, n, nnz, trow);
-    long long li, lj;
-    tile_thread_start(s, li, lj);
-    const long long li0 = li, lj0 = lj;
-    const long long rows = s.r1 - s.r0, ents = s.e1 - s.e0;
-    unsigned int flags = 0;
-    int cnt = 0;
-#pragma unroll
-    for (int k = 0; k < kPrepItemsPerThread; ++k) {
-        if (li + lj >= rows + ents) break;
-        if (li < rows && lj >= s.off[li + 1] - s.e0) {
-            ++li;
-        } else {
-            if (entry_forward(s, li, lj, deg, n, status)) { flags |= 1u << k; ++cnt; }
-            ++lj;
-        }
-    }
-    // block exclusive scan of cnt
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int incl = cnt;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        int o = __shfl_up_sync(0xffffffffu, incl, d);
-        if (lane >= d) incl += o;
-    }
-    if (lane == 31) warp_sum[warp] = incl;
-    __syncthreads();
-    int wbase = 0;
-    for (int i = 0; i < warp; ++i) wbase += warp_sum[i];
-    long long pos = tile_pre[blockIdx.x] + wbase + incl - cnt;
-    if (blockIdx.x == 0 && threadIdx.x == 0) foff[0] = 0;
-    li = li0; lj = lj0;
-#pragma unroll
-    for (int k = 0; k < kPrepItemsPerThread; ++k) {
-        if (li + lj >= rows + ents) break;
-        if (li < rows && lj >= s.off[li + 1] - s.e0) {
-            foff[s.r0 + li + 1] = pos;              // row r0+li ends here
-            ++li;
-        } else {
-            if (flags & (1u << k)) find[pos++] = s.ind[lj];
-            ++lj;
-        }
-    }
 }
 
 // This thread's items of the staged tile, classified from shared memory
@@ -412,73 +303,86 @@ __device__ __forceinline__ unsigned int forward_flags(const TileSmem &s, const T
     return flags;
 }
 
-// Pass 1: number of forward entries per tile (gather-first variant).
+// Single-pass forward-list build: every row's forward entries go to its own
+// CSR segment, find[off[v] .. off[v] + d+(v)), and d+(v) to fcnt[v].  A
+// tile places the rows it holds whole at positions from its block scan and
+// stores their counts; a row split across tiles (at most the first and the
+// last row of a tile) takes its positions for this tile's part from an
+// atomic add on fcnt[v] (zeroed by tile_bounds_kernel), so the parts of such
+// a row land in tile order of arrival.  Members keep the row's id order
+// except across those parts; sort_lists_kernel restores the order wherever
+// a consumer needs it.  With rank keys the lists hold the members' ranks.
 template <typename OffT, bool RANK>
 __global__ void __launch_bounds__(kPrepThreads)
-tile_count_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
+tile_place_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                   const int *__restrict__ key, long long n, long long nnz,
-                  const long long *__restrict__ trow,
-                  long long *__restrict__ tile_cnt, unsigned int *status)
+                  const long long *__restrict__ trow, int *__restrict__ fcnt,
+                  int *__restrict__ find, unsigned int *status)
 {
     __shared__ TileSmem s;
     __shared__ int warp_sum[kPrepThreads / 32];
-    tile_stage(s, off, ind, n, nnz, trow);
-    ThreadItems it;
-    tile_classify(s, it);
-    int rx[kPrepItemsPerThread];
-    int w = __popc(forward_flags<RANK>(s, it, key, n, status, rx));
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
-    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = w;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        long long t = 0;
-        for (int i = 0; i < kPrepThreads / 32; ++i) t += warp_sum[i];
-        tile_cnt[blockIdx.x] = t;
-    }
-}
-
-// Pass 2: write the forward adjacency (ordered stream compaction of the
-// adjacency by the forward flag) and the forward offsets foff[r+1] at every
-// row end (gather-first variant).  With rank keys the forward lists hold the
-// members' ranks (sorted afterwards by sort_lists_kernel).
-template <typename OffT, bool RANK>
-__global__ void __launch_bounds__(kPrepThreads)
-tile_fill_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
-                 const int *__restrict__ key, long long n, long long nnz,
-                 const long long *__restrict__ trow,
-                 const long long *__restrict__ tile_pre,
-                 long long *__restrict__ foff, int *__restrict__ find,
-                 unsigned int *status)
-{
-    __shared__ TileSmem s;
-    __shared__ int warp_sum[kPrepThreads / 32];
+    __shared__ int s_carry[2];
     tile_stage(s, off, ind, n, nnz, trow);
     ThreadItems it;
     tile_classify(s, it);
     int rx[kPrepItemsPerThread];
     const unsigned int flags = forward_flags<RANK>(s, it, key, n, status, rx);
     const int cnt = __popc(flags);
-    // block exclusive scan of cnt
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int incl = cnt;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-        int o = __shfl_up_sync(0xffffffffu, incl, d);
+        const int o = __shfl_up_sync(0xffffffffu, incl, d);
         if (lane >= d) incl += o;
     }
     if (lane == 31) warp_sum[warp] = incl;
-    __syncthreads();
-    int wbase = 0;
-    for (int i = 0; i < warp; ++i) wbase += warp_sum[i];
-    long long pos = tile_pre[blockIdx.x] + wbase + incl - cnt;
-    if (blockIdx.x == 0 && threadIdx.x == 0) foff[0] = 0;
+    const long long r0 = s.r0;
+    const int rows = (int)(s.r1 - s.r0);
+    const bool first_split = s.off[0] < s.e0;              // row r0 began in an earlier tile
+    const bool last_split = s.e1 > s.off[rows];            // row r1 goes on in a later tile
+    const int nloc = rows + (last_split ? 1 : 0);          // rows with items in this tile
+    __syncthreads();                                       // s.off is free from here on
+    int base = 0, total = 0;
+    for (int i = 0; i < kPrepThreads / 32; ++i) {
+        if (i < warp) base += warp_sum[i];
+        total += warp_sum[i];
+    }
+    const int pos0 = base + incl - cnt;                    // this thread's first local slot
+    int *rowbase = reinterpret_cast<int *>(s.off);         // local slot of each row's first member
+    if (threadIdx.x == 0) {
+        rowbase[0] = 0;
+        rowbase[nloc] = total;
+    }
+    int p = pos0;
 #pragma unroll
     for (int k = 0; k < kPrepItemsPerThread; ++k) {
-        if ((it.rowend_mask >> k) & 1u) {
-            foff[s.r0 + it.rowloc[k] + 1] = pos;    // the row ends here
-        } else if ((flags >> k) & 1u) {
-            find[pos++] = RANK ? rx[k] : it.x[k];
+        if ((it.rowend_mask >> k) & 1u) rowbase[it.rowloc[k] + 1] = p;
+        else if ((flags >> k) & 1u) ++p;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_carry[0] = s_carry[1] = 0;
+        if (nloc == 1 && (first_split || last_split)) {
+            s_carry[0] = atomicAdd(&fcnt[r0], rowbase[1] - rowbase[0]);
+        } else if (nloc > 1) {
+            if (first_split) s_carry[0] = atomicAdd(&fcnt[r0], rowbase[1] - rowbase[0]);
+            if (last_split)
+                s_carry[1] = atomicAdd(&fcnt[r0 + nloc - 1], rowbase[nloc] - rowbase[nloc - 1]);
+        }
+    }
+    for (int li = threadIdx.x; li < nloc; li += kPrepThreads) {
+        const bool split = (li == 0 && first_split) || (li == nloc - 1 && last_split);
+        if (!split) fcnt[r0 + li] = rowbase[li + 1] - rowbase[li];
+    }
+    __syncthreads();
+    p = pos0;
+#pragma unroll
+    for (int k = 0; k < kPrepItemsPerThread; ++k) {
+        if (!((it.rowend_mask >> k) & 1u) && ((flags >> k) & 1u)) {
+            const int li = it.rowloc[k];
+            const int carry = li == 0 ? s_carry[0] : (li == nloc - 1 ? s_carry[1] : 0);
+            find[(long long)off[r0 + li] + carry + (p - rowbase[li])] = RANK ? rx[k] : it.x[k];
+            ++p;
         }
     }
 }
@@ -556,16 +460,20 @@ __device__ void warp_sort_global(int *list, int len, int lane)
     }
 }
 
-// Sort every forward list longer than kSortMinLen ascending (rank labels).
-// Shorter lists are only ever read whole (as warp-kernel apexes, whose
-// tables do not care about order, or as short partners, whose members are
-// each checked against the apex rank), so they keep id order.  One warp per
-// 32 consecutive rows, one list at a time: in registers up to kSortRegMax
-// elements, in place beyond.  Groups come from a dynamic queue, so the few
-// groups holding several long lists do not set the kernel's length.
-__global__ void __launch_bounds__(kSortThreads)
-sort_lists_kernel(const long long *__restrict__ foff, long long n, int *__restrict__ find,
-                  Counters *ctr)
+// Sort every forward list longer than min_len ascending.  Rank labels:
+// min_len = kSortMinLen; shorter lists are only ever read whole (as
+// warp-kernel apexes, whose tables do not care about order, or as short
+// partners, whose members are each checked against the apex rank).
+// Vertex-id labels: min_len = big_hash_max, so the lists the block kernel
+// binary-searches are in id order even where a row was split across tiles.
+// One warp per 32 consecutive rows, one list at a time: in registers up to
+// kSortRegMax elements, in place beyond.  Groups come from a dynamic queue,
+// so the few groups holding several long lists do not set the kernel's
+// length.
+template <typename OffT>
+__global__ void __launch_bounds__(kSortThreads, 4)
+sort_lists_kernel(const OffT *__restrict__ off, const int *__restrict__ fcnt, long long n,
+                  int *__restrict__ find, Counters *ctr, int min_len)
 {
     const int lane = threadIdx.x & 31;
     while (true) {
@@ -575,9 +483,9 @@ sort_lists_kernel(const long long *__restrict__ foff, long long n, int *__restri
         if (v0 >= n) break;
         const long long v = v0 + lane;
         long long b = 0, e = 0;
-        if (v < n) { b = foff[v]; e = foff[v + 1]; }
+        if (v < n) { b = (long long)off[v]; e = b + fcnt[v]; }
         const long long ln = e - b;
-        unsigned int todo = __ballot_sync(0xffffffffu, ln > kSortMinLen);
+        unsigned int todo = __ballot_sync(0xffffffffu, ln > min_len);
         while (todo) {
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
@@ -598,7 +506,8 @@ sort_lists_kernel(const long long *__restrict__ foff, long long n, int *__restri
 
 // Per-vertex record and block-kernel work: rows whose forward list exceeds
 // the group kernel's table get ceil(deg / big_chunk) block items.
-__global__ void vinfo_kernel(const long long *__restrict__ foff,
+template <typename OffT>
+__global__ void vinfo_kernel(const OffT *__restrict__ off, const int *__restrict__ fcnt,
                              const int *__restrict__ deg, const int *__restrict__ rank,
                              long long n, int small_cap, int big_chunk,
                              VInfo *__restrict__ vinfo,
@@ -607,8 +516,8 @@ __global__ void vinfo_kernel(const long long *__restrict__ foff,
     long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     VInfo r;
-    r.fbeg = foff[v];
-    r.fdeg = (int)(foff[v + 1] - r.fbeg);
+    r.fbeg = (long long)off[v];
+    r.fdeg = fcnt[v];
     const int d = deg[v];
     r.key = rank ? rank[v] : d;
     vinfo[v] = r;
@@ -1317,7 +1226,7 @@ namespace {
 int g_sm_count[64];
 int g_rows_blocks[64][8];
 int g_big_blocks[64][4];
-int g_sort_blocks[64];
+int g_sort_blocks[64][2];
 
 int device_sm_count(int dev)
 {
@@ -1365,7 +1274,7 @@ Plan make_plan(long long n, long long nnz, int off_bits, bool per_vertex)
     p.o_tile = take(sizeof(long long) * (size_t)(p.n_tiles + 1));
     long long scan_n = p.n_tiles > n ? p.n_tiles : n;
     p.o_scan_tmp = take(scan_tmp_bytes(scan_n));
-    p.o_foff = take(sizeof(long long) * (size_t)(n + 1));
+    p.o_fcnt = take(sizeof(int) * (size_t)n);
     p.o_vinfo = take(sizeof(VInfo) * (size_t)n);
     p.o_find = take(sizeof(int) * (size_t)(p.fwd_cap + 4));
     p.o_tacc = take(per_vertex ? sizeof(unsigned long long) * (size_t)n : 0);
@@ -1381,9 +1290,9 @@ RowConfig pick_row_config(long long n, long long nnz)
     RowConfig c;
     const double avg = n > 0 ? (double)nnz / (double)n : 0.0;
     if (avg <= 24.0) {
-        c.group = 8; c.item_len = 256; c.prep_gather = false; c.rank_labels = false;
+        c.group = 8; c.item_len = 256; c.rank_labels = false;
     } else {
-        c.group = 32; c.item_len = 512; c.prep_gather = true; c.rank_labels = true;
+        c.group = 32; c.item_len = 512; c.rank_labels = true;
     }
     c.big_chunk = 2048;
     return c;
@@ -1413,10 +1322,10 @@ gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
 
 int launches_per_count(const RowConfig &cfg, bool per_vertex)
 {
-    // degree, tile bounds, tile count, scan x3, tile fill, vinfo, scan x3,
-    // item rows, warp kernel, block kernel, global; finalize (per vertex);
-    // rank scan, rank, list sort (rank labels)
-    return 15 + (per_vertex ? 1 : 0) + (cfg.rank_labels ? 3 : 0);
+    // degree, tile bounds, tile place, list sort, vinfo, scan x3, item rows,
+    // warp kernel, block kernel, global; finalize (per vertex); rank scan and
+    // rank (rank labels)
+    return 12 + (per_vertex ? 1 : 0) + (cfg.rank_labels ? 2 : 0);
 }
 
 template <typename OffT>
@@ -1434,7 +1343,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
     int *deg = reinterpret_cast<int *>(base + p.o_deg);
     long long *tile = reinterpret_cast<long long *>(base + p.o_tile);
     void *scan_tmp = base + p.o_scan_tmp;
-    long long *foff = reinterpret_cast<long long *>(base + p.o_foff);
+    int *fcnt = reinterpret_cast<int *>(base + p.o_fcnt);
     VInfo *vinfo = reinterpret_cast<VInfo *>(base + p.o_vinfo);
     int *find = reinterpret_cast<int *>(base + p.o_find);
     unsigned long long *tacc = reinterpret_cast<unsigned long long *>(base + p.o_tacc);
@@ -1468,38 +1377,26 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
             degree_kernel<<<vb, 256, 0, stream>>>(off, off_bits, n, deg);
         }
         tile_bounds_kernel<OffT><<<(unsigned)div_up<long long>(p.n_tiles + 1, 256), 256, 0,
-                                   stream>>>(off, n, nnz, p.n_tiles, trow);
+                                   stream>>>(off, n, nnz, p.n_tiles, trow, fcnt);
         const unsigned nt = (unsigned)p.n_tiles;
         if (rank_labels) {
-            tile_count_kernel<OffT, true><<<nt, kPrepThreads, 0, stream>>>(
-                off, ind, rank, n, nnz, trow, tile, status);
-        } else if (cfg.prep_gather) {
-            tile_count_kernel<OffT, false><<<nt, kPrepThreads, 0, stream>>>(
-                off, ind, deg, n, nnz, trow, tile, status);
+            tile_place_kernel<OffT, true><<<nt, kPrepThreads, 0, stream>>>(
+                off, ind, rank, n, nnz, trow, fcnt, find, status);
         } else {
-            tile_count_seq_kernel<OffT><<<nt, kPrepThreads, 0, stream>>>(
-                off, ind, deg, n, nnz, trow, tile, status);
+            tile_place_kernel<OffT, false><<<nt, kPrepThreads, 0, stream>>>(
+                off, ind, deg, n, nnz, trow, fcnt, find, status);
         }
-        err = exclusive_scan_i64(tile, tile, p.n_tiles, scan_tmp, stream);
-        if (err != cudaSuccess) return GTC_ERR_CUDA;
-        if (rank_labels) {
-            tile_fill_kernel<OffT, true><<<nt, kPrepThreads, 0, stream>>>(
-                off, ind, rank, n, nnz, trow, tile, foff, find, status);
-            long long sb = occupancy_blocks(sort_lists_kernel, kSortThreads, 0, dev,
-                                            &g_sort_blocks[dev & 63]);
+        {
+            long long sb = occupancy_blocks(sort_lists_kernel<OffT>, kSortThreads, 0, dev,
+                                            &g_sort_blocks[dev & 63][off_bits == 32 ? 0 : 1]);
             const long long sneed = div_up<long long>(n, 32 * (kSortThreads / 32));
             if (sneed < sb) sb = sneed;
-            sort_lists_kernel<<<(unsigned)sb, kSortThreads, 0, stream>>>(foff, n, find, ctr);
-        } else if (cfg.prep_gather) {
-            tile_fill_kernel<OffT, false><<<nt, kPrepThreads, 0, stream>>>(
-                off, ind, deg, n, nnz, trow, tile, foff, find, status);
-        } else {
-            tile_fill_seq_kernel<OffT><<<nt, kPrepThreads, 0, stream>>>(
-                off, ind, deg, n, nnz, trow, tile, foff, find, status);
+            sort_lists_kernel<OffT><<<(unsigned)sb, kSortThreads, 0, stream>>>(
+                off, fcnt, n, find, ctr, rank_labels ? kSortMinLen : cfg.big_hash_max);
         }
         const int small_cap = 4 * cfg.group;   // <= kRowSlots / 8
-        vinfo_kernel<<<vb, 256, 0, stream>>>(foff, deg, rank_labels ? rank : nullptr, n, small_cap,
-                                             cfg.big_chunk, vinfo, big);
+        vinfo_kernel<OffT><<<vb, 256, 0, stream>>>(off, fcnt, deg, rank_labels ? rank : nullptr, n,
+                                                   small_cap, cfg.big_chunk, vinfo, big);
         err = exclusive_scan_i64(big, big, n, scan_tmp, stream);
         if (err != cudaSuccess) return GTC_ERR_CUDA;
         if (timing) cudaEventRecord(timing->ev[1], stream);

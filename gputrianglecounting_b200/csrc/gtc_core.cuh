@@ -12,8 +12,7 @@ struct RowConfig {
     int item_len = 512;   // adjacency entries per dynamic work item
     int big_chunk = 2048; // adjacency entries per block-kernel item
     int big_hash_max = kBigHashMaxFdeg;  // longest list hashed by the block kernel
-    bool prep_gather = true;  // forward build: gather all degrees first (skewed graphs)
-    bool rank_labels = true;  // label vertices by degree rank (skewed graphs); implies prep_gather
+    bool rank_labels = true;  // label vertices by degree rank (skewed graphs)
 };
 
 // Kernel launches of one run_count with this configuration (the epilogue

@@ -122,7 +122,7 @@ struct Plan {
     long long fwd_cap = 0;       // capacity of the forward adjacency
     // workspace byte offsets
     size_t o_status = 0, o_counters = 0, o_deg = 0, o_tile = 0, o_scan_tmp = 0,
-           o_foff = 0, o_vinfo = 0, o_find = 0, o_tacc = 0, o_big = 0,
+           o_fcnt = 0, o_vinfo = 0, o_find = 0, o_tacc = 0, o_big = 0,
            o_bigpre = 0, o_trow = 0, o_irow = 0, o_hist = 0, o_rank = 0, o_order = 0;
     size_t bytes = 0;
 };
