@@ -461,7 +461,9 @@ __device__ void warp_sort_global(int *list, int len, int lane)
 }
 
 // Sort every forward list longer than min_len ascending.  Rank labels:
-// min_len = kSortMinLen; shorter lists are only ever read whole (as
+// min_len = min(cap, 31), cap = 4 * group the largest warp-kernel apex list;
+// the lists read in order are the block-kernel apexes' (longer than cap) and
+// the long partners' (32 or more); shorter lists are only ever read whole (as
 // warp-kernel apexes, whose tables do not care about order, or as short
 // partners, whose members are each checked against the apex rank).
 // Vertex-id labels: min_len = big_hash_max, so the lists the block kernel
@@ -1392,7 +1394,8 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
             const long long sneed = div_up<long long>(n, 32 * (kSortThreads / 32));
             if (sneed < sb) sb = sneed;
             sort_lists_kernel<OffT><<<(unsigned)sb, kSortThreads, 0, stream>>>(
-                off, fcnt, n, find, ctr, rank_labels ? kSortMinLen : cfg.big_hash_max);
+                off, fcnt, n, find, ctr,
+                rank_labels ? min(4 * cfg.group, 31) : cfg.big_hash_max);
         }
         const int small_cap = 4 * cfg.group;   // <= kRowSlots / 8
         vinfo_kernel<OffT><<<vb, 256, 0, stream>>>(off, fcnt, deg, rank_labels ? rank : nullptr, n,

@@ -56,8 +56,6 @@ constexpr int kDirectRanks = 24576;         // block kernel: one 16-bit counter 
 constexpr int kTrimLoads = 4;               // block kernel: loads in flight per partner window
 constexpr int kBitWords = 4096;             // block kernel rank bitmap: 131072 ranks
 constexpr int kBitKeys = 4096;              // longest apex list on the bitmap path
-constexpr int kSortMinLen = 16;             // lists up to this long are left unsorted
-                                            // (the smallest block-kernel cap is 4 * 4)
 
 // Error bits written to the workspace status word by device code.
 enum : unsigned int {
