@@ -1003,7 +1003,7 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
 // Block-per-row kernel for apexes whose forward list exceeds small_cap.
 // Vertex-id labels: the whole block shares one hash table of up to
 // kBigTableSlots slots (load factor <= 1/8 up to kBigTableSlots/8 keys,
-// <= 1/4 up to kBigHashMaxFdeg); beyond big_hash_max the apex list is
+// <= 1/2 up to kBigHashMaxFdeg); beyond big_hash_max the apex list is
 // binary-searched in global memory.
 // Rank labels: N+(a) lies in the ranks above the apex, (ka, n).  When that
 // range has at most kDirectRanks ranks, the block keeps one 16-bit counter

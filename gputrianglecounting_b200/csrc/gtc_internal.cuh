@@ -35,10 +35,10 @@ constexpr int kRowThreads = 256;            // warp-per-item count kernel
 constexpr int kRowSlots = 512;              // shared table slots per warp
 constexpr int kRowMinBlocks = 6;            // 48 warps per SM (register budget 42)
 constexpr int kMinItemLen = 32;             // smallest warp work item (entries)
-constexpr int kBigThreads = 512;            // block-per-row count kernel
-constexpr int kBigTableLog2 = 13;
+constexpr int kBigThreads = 256;            // block-per-row count kernel (8 blocks/SM)
+constexpr int kBigTableLog2 = 12;
 constexpr int kBigTableSlots = 1 << kBigTableLog2;   // shared hash slots (block kernel)
-constexpr int kBigHashMaxFdeg = kBigTableSlots / 4;   // load factor <= 1/4
+constexpr int kBigHashMaxFdeg = 2048;       // longest list hashed (load <= 1/2)
 
 constexpr int kScanThreads = 1024;
 
@@ -52,10 +52,10 @@ constexpr int kRankThreads = 256;           // histogram / rank kernels
 constexpr int kRankChunk = 4096;            // vertices per histogram / rank block
 constexpr int kSortThreads = 256;           // forward-list sort kernel (warp per 32 rows)
 constexpr int kSortRegMax = 1024;           // longest list sorted in registers
-constexpr int kDirectRanks = 24576;         // block kernel: one 16-bit counter per rank
+constexpr int kDirectRanks = 12288;         // block kernel: one 16-bit counter per rank
 constexpr int kTrimLoads = 4;               // block kernel: loads in flight per partner window
-constexpr int kBitWords = 4096;             // block kernel rank bitmap: 131072 ranks
-constexpr int kBitKeys = 4096;              // longest apex list on the bitmap path
+constexpr int kBitWords = 2048;             // block kernel rank bitmap: 65536 ranks
+constexpr int kBitKeys = 2048;              // longest apex list on the bitmap path
 
 // Error bits written to the workspace status word by device code.
 enum : unsigned int {
