@@ -3,7 +3,7 @@
 
 Default workload: R-MAT scale 20 (1,048,576 vertices), edge factor 16,
 (a,b,c,d) = (0.57, 0.19, 0.19, 0.05), seed 2; duplicates and self-loops
-removed, symmetrised, int64 offsets / int32 sorted adjacency; plain
+removed, symmetrised, int32 offsets / int32 sorted adjacency; plain
 (per-vertex) mode: r, t, lcc and the global count.  A step is one complete
 count of the graph (all launches of one gtc_count call) with the CSR resident
 in HBM; L2 is flushed (a 256 MiB write) before every timed step.
@@ -285,8 +285,9 @@ def run_b200(args, cfg, rank: int, world: int):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    # generated on the host (deterministic per seed, identical for both arms)
-    host = make_graph(cfg, "cpu").numpy()
+    # generated on the host (deterministic per seed, identical for both arms);
+    # int32 offsets, as the workload specifies its CSR
+    host = int32_offsets(make_graph(cfg, "cpu").numpy())
     g = host.to(dev)
     torch.cuda.synchronize()
     counter = api.TriangleCounter(dev)
@@ -369,7 +370,7 @@ def run_b200(args, cfg, rank: int, world: int):
         "dtype": "int32 ids / int64 counts", "data": "synthetic",
         "config": {"workload": args.config, "graph": cfg["label"], "n": host.n,
                    "nnz": host.nnz, "m": m, "triangles": T, "mode": "plain (r, t, lcc, global)",
-                   "offsets": "int64", "l2": f"flushed before every timed step "
+                   "offsets": "int32", "l2": f"flushed before every timed step "
                                                f"({L2_FLUSH_BYTES >> 20} MiB write)",
                    "parallelism": f"{world} independent replica(s)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -404,6 +405,15 @@ def launches_per_count(n: int, nnz: int, tuning: dict | None = None) -> int:
     return api.launch_plan(n, nnz, tuning=tuning)["launches"]
 
 
+def int32_offsets(host_graph):
+    """The same CSR with int32 offsets (the single-graph workloads specify an
+    int32 CSR; every one of them has fewer than 2^31 entries)."""
+    from gputrianglecounting_b200.graphs import CSRGraph
+    assert host_graph.nnz < (1 << 31)
+    return CSRGraph(np.ascontiguousarray(host_graph.off, dtype=np.int32), host_graph.ind,
+                    host_graph.name)
+
+
 def phase_breakdown(counter, g, flush) -> dict:
     """Per-phase device time of one count, from events the library records
     between its phases (forward build / group kernel / block kernel /
@@ -414,12 +424,13 @@ def phase_breakdown(counter, g, flush) -> dict:
     from gputrianglecounting_b200 import _lib
     fn = _lib.load().gtc_count_phase_times
     n, nnz = g.off.numel() - 1, g.ind.numel()
-    ws = counter._workspace(counter.workspace_bytes(n, nnz, 64))
+    off_bits = 32 if g.off.dtype == torch.int32 else 64
+    ws = counter._workspace(counter.workspace_bytes(n, nnz, off_bits))
     res = []
     for k in range(3):
         flush.fill_(k)
         times = (ctypes.c_float * 4)()
-        st = fn(g.off.data_ptr(), 64, g.ind.data_ptr(), n, nnz, ws.data_ptr(), ws.numel(),
+        st = fn(g.off.data_ptr(), off_bits, g.ind.data_ptr(), n, nnz, ws.data_ptr(), ws.numel(),
                 ctypes.cast(times, ctypes.c_void_p))
         _lib.check(st, "gtc_count_phase_times")
         res.append(list(times))
