@@ -460,14 +460,24 @@ __device__ void warp_sort_global(int *list, int len, int lane)
     }
 }
 
-// Sort every forward list longer than min_len ascending.  Rank labels:
-// min_len = min(cap, 31), cap = 4 * group the largest warp-kernel apex list;
-// the lists read in order are the block-kernel apexes' (longer than cap) and
+// One list of len >= 2 sorted by the whole warp.
+__device__ __forceinline__ void warp_sort_list(int *list, int len, int lane)
+{
+    if (len <= 32) warp_sort_regs<1>(list, len, lane);
+    else if (len <= 64) warp_sort_regs<2>(list, len, lane);
+    else if (len <= 128) warp_sort_regs<4>(list, len, lane);
+    else if (len <= 256) warp_sort_regs<8>(list, len, lane);
+    else if (len <= 512) warp_sort_regs<16>(list, len, lane);
+    else if (len <= kSortRegMax) warp_sort_regs<32>(list, len, lane);
+    else warp_sort_global(list, len, lane);
+}
+
+// Sort every forward list longer than min_len ascending (rank labels:
+// min_len = min(cap, 31), cap = 4 * group the largest warp-kernel apex list).
+// The lists read in order are the block-kernel apexes' (longer than cap) and
 // the long partners' (32 or more); shorter lists are only ever read whole (as
 // warp-kernel apexes, whose tables do not care about order, or as short
 // partners, whose members are each checked against the apex rank).
-// Vertex-id labels: min_len = big_hash_max, so the lists the block kernel
-// binary-searches are in id order even where a row was split across tiles.
 // One warp per 32 consecutive rows, one list at a time: in registers up to
 // kSortRegMax elements, in place beyond.  Groups come from a dynamic queue,
 // so the few groups holding several long lists do not set the kernel's
@@ -493,17 +503,32 @@ sort_lists_kernel(const OffT *__restrict__ off, const int *__restrict__ fcnt, lo
             todo &= todo - 1;
             const long long lb = __shfl_sync(0xffffffffu, b, src);
             const int len = (int)__shfl_sync(0xffffffffu, ln, src);
-            int *list = find + lb;
-            if (len <= 32) warp_sort_regs<1>(list, len, lane);
-            else if (len <= 64) warp_sort_regs<2>(list, len, lane);
-            else if (len <= 128) warp_sort_regs<4>(list, len, lane);
-            else if (len <= 256) warp_sort_regs<8>(list, len, lane);
-            else if (len <= 512) warp_sort_regs<16>(list, len, lane);
-            else if (len <= kSortRegMax) warp_sort_regs<32>(list, len, lane);
-            else warp_sort_global(list, len, lane);
+            warp_sort_list(find + lb, len, lane);
             __syncwarp();
         }
     }
+}
+
+// Vertex-id labels: restore id order in the rows whose forward entries the
+// placement split between tiles (all other rows keep the order of their
+// sorted CSR row).  One warp per tile boundary; a row holding several
+// boundaries is sorted once, by the warp of the first boundary inside it.
+template <typename OffT>
+__global__ void __launch_bounds__(kSortThreads, 4)
+sort_split_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ fcnt,
+                       const long long *__restrict__ trow, long long n_tiles, long long n,
+                       int *__restrict__ find)
+{
+    const int lane = threadIdx.x & 31;
+    const long long t = (long long)blockIdx.x * (kSortThreads / 32) + (threadIdx.x >> 5) + 1;
+    if (t >= n_tiles) return;
+    const long long r = trow[t];
+    if (r >= n) return;
+    const long long beg = (long long)off[r];
+    if (!(beg < t * kPrepTile - r)) return;                  // boundary not inside row r
+    if (t > 1 && trow[t - 1] == r && beg < (t - 1) * kPrepTile - r) return;
+    const int len = fcnt[r];
+    if (len >= 2) warp_sort_list(find + beg, len, lane);
 }
 
 // Per-vertex record and block-kernel work: rows whose forward list exceeds
@@ -1327,9 +1352,9 @@ gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
 
 int launches_per_count(const RowConfig &cfg, bool per_vertex)
 {
-    // degree, tile bounds, tile place, list sort, vinfo, scan x3, item rows,
-    // warp kernel, block kernel, global; finalize (per vertex); rank scan and
-    // rank (rank labels)
+    // degree, tile bounds, tile place, list sort (split rows with vertex
+    // ids), vinfo, scan x3, item rows, warp kernel, block kernel, global;
+    // finalize (per vertex); rank scan and rank (rank labels)
     return 12 + (per_vertex ? 1 : 0) + (cfg.rank_labels ? 2 : 0);
 }
 
@@ -1391,14 +1416,22 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
             tile_place_kernel<OffT, false><<<nt, kPrepThreads, 0, stream>>>(
                 off, ind, deg, n, nnz, trow, fcnt, find, status);
         }
-        {
+        if (rank_labels) {
+            // rank order for the lists read in order (rows hold their members
+            // in id order)
             long long sb = occupancy_blocks(sort_lists_kernel<OffT>, kSortThreads, 0, dev,
                                             &g_sort_blocks[dev & 63][off_bits == 32 ? 0 : 1]);
             const long long sneed = div_up<long long>(n, 32 * (kSortThreads / 32));
             if (sneed < sb) sb = sneed;
             sort_lists_kernel<OffT><<<(unsigned)sb, kSortThreads, 0, stream>>>(
-                off, fcnt, n, find, ctr,
-                rank_labels ? min(4 * cfg.group, 31) : cfg.big_hash_max);
+                off, fcnt, n, find, ctr, min(4 * cfg.group, 31));
+        } else if (p.n_tiles > 1) {
+            // id order (the block kernel binary-searches lists above
+            // big_hash_max): only rows split between tiles can be out of order
+            sort_split_rows_kernel<OffT><<<(unsigned)div_up<long long>(p.n_tiles - 1,
+                                                                       kSortThreads / 32),
+                                           kSortThreads, 0, stream>>>(off, fcnt, trow, p.n_tiles,
+                                                                      n, find);
         }
         const int small_cap = 4 * cfg.group;   // <= kRowSlots / 8
         vinfo_kernel<OffT><<<vb, 256, 0, stream>>>(off, fcnt, deg, rank_labels ? rank : nullptr, n,
