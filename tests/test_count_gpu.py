@@ -105,6 +105,32 @@ def test_rank_labels_large_range(cuda):
         _check(g.off, g.ind, counter.count(d_off, d_ind, tuning=tun), r_ref)
 
 
+def test_rows_split_across_many_tiles(cuda):
+    """Rows longer than one 2048-item placement tile get their forward lists
+    assembled from parts placed in any order.  K_5000: every row spans three
+    or four tiles and every forward list is long (the lowest-ranked vertex's
+    holds 4,999 members), so the list sort, the rank counters and the
+    vertex-id search path all see multi-part lists; t(v) = C(n-1, 2).  Wheel:
+    a 20,000-entry hub row whose forward list is empty, checked against the
+    oracle."""
+    n = 5000
+    off = np.arange(n + 1, dtype=np.int64) * (n - 1)
+    ind = np.concatenate([np.delete(np.arange(n, dtype=np.int32), i) for i in range(n)])
+    d_off, d_ind = _dev(off, ind, cuda)
+    counter = api.TriangleCounter(cuda)
+    for tun in (None, {"labels": 1}, {"labels": 2}, {"labels": 1, "big_hash_max": 4},
+                {"labels": 2, "group": 4}):
+        res = counter.count(d_off, d_ind, tuning=tun)
+        torch.cuda.synchronize()
+        assert (res.t.cpu().numpy() == math.comb(n - 1, 2)).all(), tun
+        assert res.triangles == math.comb(n, 3)
+    g = G.wheel(20001)
+    for off_dtype in (torch.int64, torch.int32):
+        d_off, d_ind = _dev(g.off, g.ind, cuda, off_dtype)
+        for tun in (None, {"labels": 1}, {"labels": 2}, {"labels": 1, "big_hash_max": 4}):
+            _check(g.off, g.ind, counter.count(d_off, d_ind, tuning=tun))
+
+
 def test_edge_cases(cuda):
     counter = api.TriangleCounter(cuda)
     for g in (G.from_edge_list(1, []), G.from_edge_list(9, []), G.from_edge_list(4, [(0, 3)]),
