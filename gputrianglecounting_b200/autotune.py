@@ -14,13 +14,15 @@ grids in src/param.cu:2-6).  The knobs here never change a result (tested):
                search");
   labels       the degree-ordering policy: vertex ids ordered by (degree,
                id) (1) or degree ranks with rank-sorted forward lists and the
-               block kernel's rank bitmap (2).
+               block kernel's rank bitmap (2);
+  region       warp-kernel hash slots per forward-list member (2 or 4):
+               rows per table batch against collisions.
 
 A graph's *degree profile* -- size, mean degree and skew buckets -- keys a
 cache (in memory and, optionally, a JSON file), so each profile is tuned
 once.  Each candidate is timed with CUDA events on the device (best of a few
 runs after a warm-up).  search="grid" times every combination; "staged"
-first picks labels x group with the other knobs at the library's choice,
+first picks labels x group x region with the other knobs at the library's choice,
 then item_len x big_chunk under that choice (for inputs whose single count
 takes long, such as a whole batch).
 """
@@ -38,11 +40,12 @@ from . import api
 
 DEFAULT_GRID = {
     "labels": (1, 2),
+    "region": (2, 4),
     "group": (8, 16, 32),
     "item_len": (128, 256, 512, 1024),
     "big_chunk": (1024, 2048, 4096),
 }
-STAGES = (("labels", "group"), ("item_len", "big_chunk"))
+STAGES = (("labels", "group", "region"), ("item_len", "big_chunk"))
 
 _lock = threading.Lock()
 _memory: dict[str, dict] = {}

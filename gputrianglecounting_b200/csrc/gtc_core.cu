@@ -854,7 +854,8 @@ __device__ __forceinline__ void region_insert(int *keys, int toff, int lg, int k
 // from a dynamic queue; the warp handles all rows of the item together,
 // up to 32 rows at a time, with warp-uniform control flow:
 //   1. one lane per row loads the row's segment and record; each active row
-//      gets its own region (2^ceil(log2(4 d+)) slots, load factor <= 1/4) of
+//      gets its own region (2^ceil(log2(m d+)) slots, m = region_mult: load
+//      factor <= 1/2 for low-degree graphs, <= 1/4 otherwise) of
 //      the warp's shared table, placed by a prefix scan (rows that do not fit
 //      wait for the next batch);
 //   2. the rows' forward lists are inserted as one flattened stream;
@@ -871,7 +872,7 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                   const int *__restrict__ find,
                   unsigned long long *__restrict__ tacc, Counters *ctr,
                   unsigned int *status, const long long *__restrict__ irow,
-                  long long n_items, int item_len, int small_cap,
+                  long long n_items, int item_len, int small_cap, int region_mult,
                   const int *__restrict__ order)
 {
     constexpr int kWarps = kRowThreads / 32;
@@ -903,7 +904,7 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
             VInfo vi{0, 0, 0};
             if (len > 0) vi = vinfo[r];
             bool act = len > 0 && vi.fdeg > 0 && vi.fdeg <= small_cap;
-            const int lg = act ? max(ceil_log2(4 * (long long)vi.fdeg), 2) : 0;
+            const int lg = act ? max(ceil_log2((long long)region_mult * vi.fdeg), 2) : 0;
             const int ts = act ? (1 << lg) : 0;
             const int tincl = warp_incl_scan(ts);
             const int toff = tincl - ts;
@@ -1317,7 +1318,7 @@ RowConfig pick_row_config(long long n, long long nnz)
     RowConfig c;
     const double avg = n > 0 ? (double)nnz / (double)n : 0.0;
     if (avg <= 24.0) {
-        c.group = 8; c.item_len = 256; c.rank_labels = false;
+        c.group = 8; c.item_len = 256; c.rank_labels = false; c.region_mult = 2;
     } else {
         c.group = 32; c.item_len = 512; c.rank_labels = true;
     }
@@ -1340,13 +1341,15 @@ gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
     if (tuning->item_len < 0 || (tuning->item_len > 0 && tuning->item_len < kMinItemLen) ||
         tuning->big_chunk < 0 || tuning->big_hash_max < 0 ||
         tuning->big_hash_max > kBigHashMaxFdeg || tuning->big_chunk > 32768 ||
-        tuning->labels < 0 || tuning->labels > 2)
+        tuning->labels < 0 || tuning->labels > 2 ||
+        (tuning->region != 0 && tuning->region != 2 && tuning->region != 4))
         return GTC_ERR_INVALID_ARGUMENT;
     if (tuning->item_len) cfg.item_len = tuning->item_len;
     if (tuning->big_chunk) cfg.big_chunk = tuning->big_chunk;
     if (tuning->big_hash_max) cfg.big_hash_max = tuning->big_hash_max;
     if (tuning->labels == GTC_LABELS_VERTEX_ID) cfg.rank_labels = false;
     if (tuning->labels == GTC_LABELS_DEGREE_RANK) cfg.rank_labels = true;
+    if (tuning->region) cfg.region_mult = tuning->region;
     return GTC_OK;
 }
 
@@ -1451,7 +1454,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                 if (need < blocks) blocks = (int)need;
                 kern<<<blocks, kRowThreads, 0, stream>>>(off, ind, n, nnz, vinfo, find, tacc, ctr,
                                                          status, irow, n_items, cfg.item_len,
-                                                         small_cap, lorder);
+                                                         small_cap, cfg.region_mult, lorder);
             };
             if (per_vertex) launch_rows(count_rows_kernel<true, OffT>);
             else launch_rows(count_rows_kernel<false, OffT>);

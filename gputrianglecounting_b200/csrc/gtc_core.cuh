@@ -13,6 +13,8 @@ struct RowConfig {
     int big_chunk = 2048; // adjacency entries per block-kernel item
     int big_hash_max = kBigHashMaxFdeg;  // longest list hashed by the block kernel
     bool rank_labels = true;  // label vertices by degree rank (skewed graphs)
+    int region_mult = 4;      // warp kernel: table slots per forward member (2 or 4);
+                              // low-degree graphs fit twice the rows per batch with 2
 };
 
 // Kernel launches of one run_count with this configuration (the epilogue

@@ -110,6 +110,8 @@ gtc_status gtc_count(const void *d_off, int off_bits, const int32_t *d_ind,
  *                (degree, id)), 2 = degree ranks (vertices counting-sorted
  *                by degree, lists sorted by rank, block kernel on a rank
  *                bitmap); the library picks ranks for mean degree > 24
+ *   region       warp-kernel hash slots per forward-list member: 2 or 4 (the
+ *                library picks 2 for mean degree <= 24, else 4)
  */
 typedef struct gtc_tuning {
     int group;
@@ -117,6 +119,7 @@ typedef struct gtc_tuning {
     int big_chunk;
     int big_hash_max;
     int labels;
+    int region;
 } gtc_tuning;
 
 /* Values of gtc_tuning.labels. */

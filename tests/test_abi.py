@@ -82,6 +82,9 @@ def test_invalid_arguments_rejected_before_any_device_work():
     bad = _lib.Tuning(group=12)
     assert lib.gtc_count_tuned(fake, 32, fake, 10, 4, 0, None, None, None, None, fake, 1 << 20,
                                None, ctypes.byref(bad)) == 1
+    bad = _lib.Tuning(region=3)
+    assert lib.gtc_count_tuned(fake, 32, fake, 10, 4, 0, None, None, None, None, fake, 1 << 20,
+                               None, ctypes.byref(bad)) == 1
     bad = _lib.Tuning(labels=5)
     assert lib.gtc_count_tuned(fake, 32, fake, 10, 4, 0, None, None, None, None, fake, 1 << 20,
                                None, ctypes.byref(bad)) == 1

@@ -13,7 +13,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-_SHAPES = [{}, {"group": 4}, {"group": 8}, {"group": 16}, {"group": 32},
+_SHAPES = [{}, {"group": 4}, {"group": 8}, {"group": 16, "region": 2}, {"group": 32, "region": 2},
            {"group": 8, "item_len": 64, "big_chunk": 128},
            {"group": 4, "big_hash_max": 8},     # block kernel's in-place search path
            {"group": 32, "item_len": 32, "big_chunk": 32, "big_hash_max": 16}]
