@@ -61,7 +61,7 @@ CONFIGS = {
 # dram__bytes_write.sum, cold L2 before each launch).  Far below B_alg: the
 # forward lists and the per-vertex records stay in the 126 MB L2, so most
 # probe reads never reach HBM.
-DRAM_TRAFFIC = {"rmat20": 1475482880, "rgg": 1422157312}
+DRAM_TRAFFIC = {"rmat20": 1475482880, "rgg": 1422522880}
 
 
 def make_graph(cfg: dict, device):
