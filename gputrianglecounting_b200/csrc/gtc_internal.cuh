@@ -2,21 +2,25 @@
 //
 // Algorithm (same output as the reference's per-vertex kernel,
 // src/clusteringCount.cu:314-359, computed differently):
-//   1. orient every undirected edge from the lower to the higher
-//      (degree, id) rank and build the forward lists N+(v) (a filtered copy
-//      of the sorted adjacency, so every N+(v) stays sorted);
-//   2. give every oriented edge u->v to its "apex": the endpoint with the
-//      longer forward list (ties to the source u).  The apex's N+ is staged in
-//      a shared-memory hash table and the partner's (shorter) N+ is probed
-//      into it, so each triangle {u,v,w} is found exactly once, at the edge
-//      between its two lowest-ranked vertices, with sum over edges of
-//      min(d+(u), d+(v)) probes in total;
+//   1. order the vertices by degree -- as (degree, id) with vertex-id labels,
+//      or by a counting sort into ranks with degree-rank labels -- orient
+//      every undirected edge from its lower to its higher end and build the
+//      forward lists N+(v) in one pass, each at the start of v's own CSR
+//      segment (holding ids or ranks); lists a consumer reads in order are
+//      sorted;
+//   2. give every oriented edge one "apex" that intersects for it: the end
+//      with the longer forward list (ties to the source), except that with
+//      rank labels a block-kernel apex owns every edge to a lower-ranked
+//      neighbour.  The apex's N+ is staged in shared memory (hash table, rank
+//      bitmap or per-rank counters) and the partner's N+ is probed into it,
+//      so each triangle {u,v,w} is found exactly once, at the edge between
+//      its two lowest-ordered vertices;
 //   3. credit the triangle to all three vertices: the apex through a register
-//      count, the partner through a per-partner shared counter, the third
-//      vertex w through a per-slot shared hit counter that is flushed to
-//      global memory once per (apex, w).
+//      or block count, the partner through a warp reduction or a ballot
+//      popcount, the third vertex w through a shared per-member hit counter
+//      flushed to global memory once per (apex, w).
 // All counting is integer and exact; the result does not depend on the
-// order in which blocks run.
+// order in which blocks run, on the labels or on the order of equal degrees.
 #pragma once
 
 #include <cstdint>
