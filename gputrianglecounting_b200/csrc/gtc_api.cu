@@ -61,16 +61,27 @@ __global__ void validate_rows_kernel(const OffT *__restrict__ off,
 template <typename OffT>
 __global__ void validate_symmetry_kernel(const OffT *__restrict__ off,
                                          const int *__restrict__ ind, long long n,
-                                         int *reason)
+                                         int *reason, unsigned long long *counts)
 {
+    // Rows are strictly ascending without self-loops (checked before), so
+    // reversal maps the entries (a, x) with a < x injectively onto those with
+    // a > x: the graph is symmetric iff every such upper entry's reverse is
+    // present and both kinds are equally many (counts[0] vs counts[1]).  Only
+    // upper entries are searched for, half of all entries.
     if (*(volatile int *)reason != kNoReason) return;
     const int lane = threadIdx.x & 31;
     const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    unsigned long long upper = 0, lower = 0;
     for (long long a = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < n; a += warps) {
         const long long rb = off[a], re = off[a + 1];
         bool ok = true;
         for (long long e = rb + lane; e < re; e += 32) {
             const int x = ind[e];
+            if (x < a) {
+                ++lower;
+                continue;
+            }
+            ++upper;
             long long lo = off[x], hi = off[x + 1];
             while (lo < hi) {
                 long long mid = (lo + hi) >> 1;
@@ -80,6 +91,15 @@ __global__ void validate_symmetry_kernel(const OffT *__restrict__ off,
         }
         if (!__all_sync(0xffffffffu, ok) && lane == 0) atomicMin(reason, GTC_CSR_ASYMMETRIC);
     }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        upper += __shfl_down_sync(0xffffffffu, upper, d);
+        lower += __shfl_down_sync(0xffffffffu, lower, d);
+    }
+    if (lane == 0) {
+        if (upper) atomicAdd(&counts[0], upper);
+        if (lower) atomicAdd(&counts[1], lower);
+    }
 }
 
 template <typename OffT>
@@ -87,7 +107,11 @@ gtc_status run_validate(const OffT *off, const int *ind, long long n, long long 
                         void *ws, int32_t *h_reason, cudaStream_t stream)
 {
     int *reason = static_cast<int *>(ws);
+    unsigned long long *counts =
+        reinterpret_cast<unsigned long long *>(static_cast<char *>(ws) + 64);
     cudaError_t e = cudaMemsetAsync(reason, 0x7f, sizeof(int), stream);
+    if (e != cudaSuccess) return GTC_ERR_CUDA;
+    e = cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return GTC_ERR_CUDA;
     const unsigned vb = (unsigned)div_up<long long>(n + 1, 256);
     validate_offsets_kernel<<<vb, 256, 0, stream>>>(off, n, nnz, reason);
@@ -98,14 +122,20 @@ gtc_status run_validate(const OffT *off, const int *ind, long long n, long long 
         long long want = div_up<long long>(n, 8);
         unsigned blocks = (unsigned)(want < (long long)sms * 16 ? want : (long long)sms * 16);
         validate_rows_kernel<<<blocks, 256, 0, stream>>>(off, ind, n, reason);
-        validate_symmetry_kernel<<<blocks, 256, 0, stream>>>(off, ind, n, reason);
+        validate_symmetry_kernel<<<blocks, 256, 0, stream>>>(off, ind, n, reason, counts);
     }
-    int host = 0;
-    e = cudaMemcpyAsync(&host, reason, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    // reason word and the two entry counts in one read
+    unsigned char host[80];
+    e = cudaMemcpyAsync(host, ws, sizeof(host), cudaMemcpyDeviceToHost, stream);
     if (e != cudaSuccess) return GTC_ERR_CUDA;
     e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return GTC_ERR_CUDA;
-    *h_reason = host == kNoReason ? GTC_CSR_OK : host;
+    int r = 0;
+    unsigned long long c[2] = {0, 0};
+    std::memcpy(&r, host, sizeof(int));
+    std::memcpy(c, host + 64, sizeof(c));
+    if (r == kNoReason && c[0] != c[1]) r = GTC_CSR_ASYMMETRIC;
+    *h_reason = r == kNoReason ? GTC_CSR_OK : r;
     return GTC_OK;
 }
 

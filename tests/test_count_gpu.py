@@ -197,7 +197,8 @@ def test_compat_kernelCall(cuda):
 
 
 @pytest.mark.parametrize("defect,reason", [
-    ("ok", 0), ("offsets", 1), ("range", 2), ("selfloop", 3), ("unsorted", 4), ("asym", 5)])
+    ("ok", 0), ("offsets", 1), ("range", 2), ("selfloop", 3), ("unsorted", 4), ("asym", 5),
+    ("asym_lower", 5), ("ok_rmat", 0)])
 def test_validate_csr(cuda, defect, reason):
     g = G.complete(6).numpy()
     off, ind = g.off.copy(), g.ind.copy()
@@ -211,6 +212,13 @@ def test_validate_csr(cuda, defect, reason):
         ind[0], ind[1] = ind[1], ind[0]
     elif defect == "asym":
         off = np.array([0, 1, 2, 3], np.int64); ind = np.array([1, 2, 0], np.int32)
+    elif defect == "asym_lower":
+        # every entry (a, x) with a < x has its reverse; the extra (2, 0) has
+        # none, which only the count of such entries reveals
+        off = np.array([0, 1, 2, 3], np.int64); ind = np.array([1, 0, 0], np.int32)
+    elif defect == "ok_rmat":
+        h = G.rmat(14, 16, 9).numpy()
+        off, ind = np.asarray(h.off, np.int64), np.asarray(h.ind, np.int32)
     for off_dtype in (torch.int64, torch.int32):
         d_off, d_ind = _dev(off, ind, cuda, off_dtype)
         assert api.validate_csr(d_off, d_ind)[0] == reason
