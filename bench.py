@@ -34,6 +34,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "per-vertex TC edges/s"
 UNIT = "undirected edges/s"
+DTYPE = "int32 ids / int64 counts"
 L2_FLUSH_BYTES = 256 << 20
 
 CONFIGS = {
@@ -57,11 +58,22 @@ CONFIGS = {
 
 
 # DRAM bytes (read + write) of one complete count, summed over its launches
-# from one ncu capture of this same workload (dram__bytes_read.sum +
-# dram__bytes_write.sum, cold L2 before each launch).  Far below B_alg: the
-# forward lists and the per-vertex records stay in the 126 MB L2, so most
-# probe reads never reach HBM.
-DRAM_TRAFFIC = {"rmat20": 1475482880, "rgg": 1422522880}
+# from one ncu capture of the same workload (dram__bytes_read.sum +
+# dram__bytes_write.sum, cold L2 before each launch), read from the committed
+# summary profiles/dram_per_kernel_<workload>.md (its "traffic per count:"
+# line).  Far below B_alg: the forward lists and the per-vertex records stay
+# in the 126 MB L2, so most probe reads never reach HBM.
+def dram_traffic(workload: str) -> dict | None:
+    path = os.path.join(ROOT, "profiles", f"dram_per_kernel_{workload}.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic per count:"):
+                    parts = line.split(":", 1)[1].split()
+                    return {"bytes": int(parts[0].replace(",", "")), "source": os.path.relpath(path, ROOT)}
+    except OSError:
+        pass
+    return None
 
 
 def make_graph(cfg: dict, device):
@@ -71,6 +83,14 @@ def make_graph(cfg: dict, device):
     if cfg["kind"] == "er":
         return G.erdos_renyi(cfg["n"], cfg["deg"], cfg["seed"], device=device)
     return G.rgg2d(cfg["n"], cfg["deg"], cfg["seed"], device=device)
+
+
+def graph_config(workload: str, cfg: dict, g, world: int) -> dict:
+    """The `config` object of a single-graph line (identical for both arms)."""
+    return {"workload": workload, "graph": cfg["label"], "n": g.n, "nnz": g.nnz, "m": g.m,
+            "mode": "plain (r, t, lcc, global)", "offsets": "int32",
+            "l2": f"GPU arm: flushed before every timed step ({L2_FLUSH_BYTES >> 20} MiB write)",
+            "parallelism": f"{world} independent replica(s)"}
 
 
 def algorithmic_bytes(host_graph) -> dict:
@@ -151,48 +171,130 @@ class ClockSampler:
 
 # --------------------------------------------------------------- reference
 
-def reference_sample_rows(host_graph, stride: int, phase: int = 0) -> np.ndarray:
-    """Systematic sample of rows in degree order (every stride-th row), so the
-    sample holds its share of hub rows and low-degree rows alike."""
-    deg = np.diff(host_graph.off)
-    order = np.argsort(deg, kind="stable")
-    return np.ascontiguousarray(order[phase % stride::stride], dtype=np.int64)
+class ReferenceTimer:
+    """The reference's CPU count timed on the host cores: count_all_trianglesCPU
+    (vertex-list overload, src/clusteringCount.cpp:125-155, compiled unchanged
+    into oracle/_ref) on the workload's int32 CSR, row by row, with the rows
+    spread over all host threads by OpenMP (dynamic, 1) in units: each heavy
+    row (cost >= total / (256 threads)) is a unit of its own, the other rows
+    form units of up to 64 consecutive ids (the granularity of a
+    schedule(dynamic, 64) row loop).  Per-unit times are measured, so the
+    full-graph wall time can be estimated without running the whole graph
+    every step:
+
+        T_full = max((sum of heavy-unit times + k * sum of sampled light-unit
+                      times) / threads, largest unit time)
+
+    which is the lower bound of any schedule on `threads` cores (optimistic
+    for the reference).  The heavy units are measured once (calibrate);
+    each step times a systematic 1-in-k sample of the light units in order
+    of cost (phase = step index), k chosen so a step lasts about step_s.
+    A graph whose whole count fits in step_s runs whole every step, and
+    T_full is simply its wall time.  Unit cost model (merge steps of the
+    reference's count_intersectionsReg for a row): d(v)^2 + sum_{u in N(v)} d(u).
+    """
+
+    CHUNK = 64
+
+    def __init__(self, host_graph, threads: int, step_s: float = 2.0):
+        from oracle import oracle as O
+        self.O = O
+        self.threads = threads
+        self.step_s = step_s
+        off = np.asarray(host_graph.off, np.int64)
+        self.off32 = np.ascontiguousarray(off, np.int32)
+        self.ind32 = np.ascontiguousarray(host_graph.ind, np.int32)
+        self.m = host_graph.m
+        n = off.shape[0] - 1
+        deg = np.diff(off).astype(np.float64)
+        row = np.repeat(np.arange(n, dtype=np.int64), np.diff(off))
+        cost = deg * deg + np.bincount(row, weights=deg[self.ind32], minlength=n) + 1.0
+        total = float(cost.sum())
+        heavy = np.nonzero(cost >= total / (256.0 * threads))[0]
+        heavy = heavy[np.argsort(-cost[heavy], kind="stable")]
+        is_heavy = np.zeros(n, bool)
+        is_heavy[heavy] = True
+        light_rows = np.nonzero(~is_heavy)[0]
+        chunk_of = light_rows // self.CHUNK
+        starts = np.nonzero(np.r_[True, chunk_of[1:] != chunk_of[:-1]])[0] if n else np.zeros(0, int)
+        # unit table: heavy rows one per unit, then the light chunks
+        self.unit_rows = np.concatenate([heavy, light_rows]).astype(np.int64)
+        self.unit_off = np.concatenate([np.arange(heavy.shape[0] + 1),
+                                        heavy.shape[0] + np.r_[starts[1:], light_rows.shape[0]]]
+                                       ).astype(np.int64) if n else np.zeros(1, np.int64)
+        self.n_heavy = int(heavy.shape[0])
+        light_cost = np.add.reduceat(cost[light_rows], starts) if light_rows.size else np.zeros(0)
+        self.light_units = self.n_heavy + np.argsort(-light_cost, kind="stable")   # cost order
+        self.cost_heavy = float(cost[heavy].sum())
+        self.cost_light = float(light_cost.sum())
+        self.tri = np.zeros(self.ind32.shape[0], np.int64)
+        self.r = np.zeros(n, np.int64)
+        self.whole = False
+        self.k = 1
+        self.heavy_ns = np.zeros(0, np.int64)
+        self.heavy_wall = 0.0
+
+    def _run(self, units):
+        t0 = time.perf_counter()
+        ns, _ = self.O.ref_units_timed(self.off32, self.ind32, self.unit_rows, self.unit_off,
+                                       units, self.threads, tri=self.tri, r=self.r)
+        return ns, time.perf_counter() - t0
+
+    def calibrate(self) -> None:
+        """Time the heavy units once and a pilot light sample; choose k."""
+        heavy_units = np.arange(self.n_heavy, dtype=np.int64)
+        if self.n_heavy:
+            self.heavy_ns, self.heavy_wall = self._run(heavy_units)
+        nl = self.light_units.shape[0]
+        pilot_k = max(1, nl // 512)
+        ns, _ = self._run(self.light_units[::pilot_k])
+        sample_cost = self.cost_light / pilot_k if nl else 0.0
+        rate = (ns.sum() / sample_cost) if sample_cost > 0 else 0.0          # ns per cost unit
+        light_est_s = rate * self.cost_light / 1e9
+        heavy_s = self.heavy_ns.sum() / 1e9
+        est_whole = max((heavy_s + light_est_s) / self.threads,
+                        self.heavy_ns.max() / 1e9 if self.n_heavy else 0.0)
+        if est_whole <= self.step_s:
+            self.whole = True
+            self.k = 1
+        else:
+            self.k = max(1, int(math.ceil(light_est_s / self.threads / self.step_s)))
+
+    def step(self, index: int) -> dict:
+        """One timed step; returns its wall time and the full-graph estimate."""
+        if self.whole:
+            units = np.arange(self.unit_off.shape[0] - 1, dtype=np.int64)
+            ns, wall = self._run(units)
+            return {"wall_s": wall, "full_s": wall, "units": int(units.shape[0])}
+        units = self.light_units[index % self.k::self.k]
+        ns, wall = self._run(units)
+        hv = self.heavy_ns
+        serial = hv.sum() + self.k * ns.sum()
+        longest = max(hv.max() if hv.size else 0, ns.max() if ns.size else 0)
+        full = max(serial / self.threads, longest) / 1e9
+        return {"wall_s": wall, "full_s": full, "units": int(units.shape[0])}
+
+    def describe(self) -> str:
+        if self.whole:
+            return (f"the whole graph every step: the reference's count_all_trianglesCPU "
+                    f"(vertex-list overload, int32 CSR) over all rows, OpenMP dynamic over "
+                    f"{self.unit_off.shape[0] - 1} units on {self.threads} threads")
+        return (f"the reference's count_all_trianglesCPU (vertex-list overload, int32 CSR) on "
+                f"{self.threads} threads; {self.n_heavy} heavy rows (one unit each) timed once "
+                f"({self.heavy_wall:.2f} s wall), then each step a systematic 1-in-{self.k} "
+                f"sample of the {self.light_units.shape[0]} light 64-row units in cost order; "
+                f"full-graph time = max((heavy + {self.k} x sampled unit time) / threads, "
+                f"longest unit), a lower bound for any schedule")
 
 
-def time_reference_sample(prep, host_graph, stride, phase, threads):
-    from oracle import oracle as O
-    off64, ind64 = prep
-    rows = reference_sample_rows(host_graph, stride, phase)
-    tri = np.zeros(ind64.shape[0], np.int64)
-    r = np.zeros(off64.shape[0] - 1, np.int64)
-    t0 = time.perf_counter()
-    O.ref_rows_prepared(off64, ind64, rows, tri, r, threads)
-    dt = time.perf_counter() - t0
-    return dt, rows.shape[0]
-
-
-def calibrate_stride(prep, host_graph, threads, target_s: float) -> int:
-    """Pick the sampling stride so one sample takes about target_s seconds."""
-    n = host_graph.n
-    stride = max(1, n // 2000)
-    while True:
-        dt, _ = time_reference_sample(prep, host_graph, stride, 0, threads)
-        if dt > 0.2 or stride == 1:
-            break
-        stride = max(1, stride // 8)
-    est_full = dt * stride
-    return max(1, min(n, int(math.ceil(est_full / target_s)))), est_full
-
-
-def cpu_baseline(host_graph, threads: int, target_s: float = 4.0) -> dict:
-    from oracle import oracle as O
-    prep = O.ref_prepared(host_graph.off, host_graph.ind)
-    stride, _ = calibrate_stride(prep, host_graph, threads, target_s)
-    dt, rows = time_reference_sample(prep, host_graph, stride, 1, threads)
-    full = dt * stride
-    return {"value": host_graph.m / full, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"rows {rows} of {host_graph.n} (every {stride}-th row in degree order), "
-                      f"{dt:.2f} s; full-graph time estimated as sample x {stride} = {full:.1f} s"}
+def cpu_baseline(host_graph, threads: int) -> dict:
+    """The reference's CPU count on this host (calibration + one sampled step)."""
+    rt = ReferenceTimer(host_graph, threads)
+    rt.calibrate()
+    st = rt.step(0)
+    return {"value": host_graph.m / st["full_s"], "unit": UNIT, "cores": threads,
+            "kind": "reference", "sample": rt.describe(),
+            "full_graph_s_estimate": st["full_s"], "step_wall_s": st["wall_s"]}
 
 
 def run_reference(args, cfg, rank: int) -> None:
@@ -204,31 +306,29 @@ def run_reference(args, cfg, rank: int) -> None:
     if cfg["kind"] in ("batched", "serving"):
         run_reference_batched(args, CONFIGS["batched"], threads)
         return
-    g = make_graph(cfg, "cpu").numpy()
-    prep = O.ref_prepared(g.off, g.ind)
-    stride, _ = calibrate_stride(prep, g, threads, 2.0)
+    g = int32_offsets(make_graph(cfg, "cpu").numpy())
+    rt = ReferenceTimer(g, threads)
+    t0 = time.perf_counter()
+    rt.calibrate()
+    calib_s = time.perf_counter() - t0
     for w in range(args.warmup):
-        time_reference_sample(prep, g, stride, w, threads)
-    est = []
-    rows_total = 0
-    for k in range(args.steps):
-        dt, rows = time_reference_sample(prep, g, stride, args.warmup + k, threads)
-        est.append(dt * stride)
-        rows_total += rows
-    full = statistics.mean(est)
+        rt.step(w)
+    steps = [rt.step(args.warmup + k) for k in range(args.steps)]
+    full = statistics.mean(st["full_s"] for st in steps)
+    wall = statistics.mean(st["wall_s"] for st in steps)
     value = g.m / full
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": full * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": args.config, "graph": cfg["label"], "n": g.n, "nnz": g.nnz,
-                   "m": g.m, "mode": "per-vertex (row sums of triNE)"},
+        "ms_per_step": wall * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": DTYPE, "data": "synthetic",
+        "config": graph_config(args.config, cfg, g, world=args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"each step: every {stride}-th row in degree order "
-                                   f"(~{rows_total // max(1, args.steps)} rows) through the "
-                                   f"reference's count_all_trianglesCPU vertex-list overload, "
-                                   f"OpenMP dynamic,64; full-graph time = sample x {stride}"},
+                         "sample": rt.describe(), "full_graph_s_estimate": full,
+                         "calibration_s": calib_s},
+        "reference_timing": {"ms_per_step": "wall time of each step's sample",
+                             "value": "undirected edges / estimated full-graph time",
+                             "full_graph_ms_estimate": full * 1e3},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -274,7 +374,7 @@ def run_reference_batched(args, cfg, threads: int) -> None:
 
 # ------------------------------------------------------------------ b200
 
-def run_b200(args, cfg, rank: int, world: int):
+def run_b200(args, name: str, rank: int, world: int, with_baseline: bool = True):
     import torch
     import torch.distributed as dist
     from gputrianglecounting_b200 import api
@@ -282,6 +382,7 @@ def run_b200(args, cfg, rank: int, world: int):
     from gputrianglecounting_b200._lib import load as load_lib
     load_lib()
 
+    cfg = CONFIGS[name]
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -361,21 +462,21 @@ def run_b200(args, cfg, rank: int, world: int):
     value = edges_all / (total_ms / 1e3)
     ms_per_step = total_ms / args.steps
     work = algorithmic_bytes(host)
+    traffic = dram_traffic(name)
     peak, peak_kind = measured_peaks()
     achieved = work["B_alg"] / (ms_per_step / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "int32 ids / int64 counts", "data": "synthetic",
-        "config": {"workload": args.config, "graph": cfg["label"], "n": host.n,
-                   "nnz": host.nnz, "m": m, "triangles": T, "mode": "plain (r, t, lcc, global)",
-                   "offsets": "int32", "l2": f"flushed before every timed step "
-                                               f"({L2_FLUSH_BYTES >> 20} MiB write)",
-                   "parallelism": f"{world} independent replica(s)"},
+        "dtype": DTYPE, "data": "synthetic",
+        "config": graph_config(name, cfg, host, world),
+        "result": {"triangles": T},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": DRAM_TRAFFIC.get(args.config),
-                     "traffic_unit": "bytes per count (ncu capture of this workload)",
+                     "frac": achieved / peak,
+                     "traffic": (traffic or {}).get("bytes"),
+                     "traffic_unit": "bytes per count (ncu capture of this workload: "
+                                     f"{(traffic or {}).get('source')})",
                      "scope": "one complete count (all launches of one gtc_count call)",
                      "work_model": f"B_alg = 4W + 4(n+1) + 4nnz + 16n = {work['B_alg']} bytes, "
                                    f"W = sum_undirected min(d_u, d_v) = {work['W']}",
@@ -392,7 +493,7 @@ def run_b200(args, cfg, rank: int, world: int):
         "clocks": clk.result,
         "gpu_launches": launches_per_count(host.n, host.nnz) * args.steps,
     }
-    if not args.no_cpu_baseline:
+    if with_baseline and not args.no_cpu_baseline:
         from oracle import oracle as O
         line["cpu_baseline"] = cpu_baseline(host, O.max_threads())
     return line
@@ -500,12 +601,16 @@ def run_batched(args, cfg, rank: int, world: int):
     total_ms = gdist.max_over_ranks(sum(step_ms), dev)
     graph_T = out.graph_T.clone()
 
-    # one call per graph, same engine, same outputs
+    # one call per graph, same engine, same outputs (views of one buffer per
+    # output, so that the whole result compares in one go)
     tc = api.TriangleCounter(dev)
-    per = [api.TriangleCounts(r=torch.empty(g.n, dtype=torch.int64, device=dev), t=None,
-                              lcc=torch.empty(g.n, dtype=torch.float64, device=dev),
-                              global_counts=torch.empty(3, dtype=torch.int64, device=dev))
-           for g in graphs]
+    r_one = torch.empty_like(out.r)
+    lcc_one = torch.empty_like(out.lcc)
+    g_one = torch.empty(len(graphs), 3, dtype=torch.int64, device=dev)
+    vs = batch.vstart.cpu().tolist()
+    per = [api.TriangleCounts(r=r_one[vs[i]:vs[i + 1]], t=None, lcc=lcc_one[vs[i]:vs[i + 1]],
+                              global_counts=g_one[i])
+           for i in range(len(graphs))]
     for g, o in zip(graphs, per):                      # warm-up: workspace, caches
         tc.count(g.off, g.ind, out=o)
     torch.cuda.synchronize()
@@ -518,8 +623,11 @@ def run_batched(args, cfg, rank: int, world: int):
         b.record()
         torch.cuda.synchronize()
         base_ms.append(a.elapsed_time(b))
-    per_T = torch.stack([o.global_counts[0] for o in per])
-    assert torch.equal(per_T, graph_T), "batched and per-graph counts differ"
+    # every per-vertex r and lcc and every per-graph T of the batch equals the
+    # graph counted alone
+    assert torch.equal(g_one[:, 0], graph_T), "batched and per-graph T differ"
+    assert torch.equal(r_one, out.r), "batched and per-graph r differ"
+    assert torch.equal(lcc_one.view(torch.int64), out.lcc.view(torch.int64)), "lcc differ"
     del graph
     if rank != 0:
         return None
@@ -651,12 +759,24 @@ def main() -> None:
         elif args.config == "serving":
             line = run_serving(args, cfg, rank, world)
         else:
-            line = run_b200(args, cfg, rank, world)
+            line = run_b200(args, args.config, rank, world)
             if args.config == "rmat20" and not args.no_extras:
-                # the headline metric's other two parts: batched speedup and
-                # served latency, each from its own workload
+                # the other single-graph workloads, each with its own roofline
+                # and CPU baseline, then the headline metric's other two parts:
+                # batched speedup and served latency
                 sub = argparse.Namespace(**vars(args))
-                sub.steps, sub.warmup = 5, 3
+                sub.steps, sub.warmup = 20, 3
+                for other in ("rgg", "er"):
+                    o = run_b200(sub, other, rank, world)
+                    if line is not None:
+                        line[other] = {"edges_per_s": o["value"], "ms": o["ms_per_step"],
+                                       "steps": o["steps"], "config": o["config"],
+                                       "result": o["result"], "roofline": o["roofline"],
+                                       "phases_ms": o["phases_ms"], "e2e": o["e2e"],
+                                       "clocks": o["clocks"]}
+                        if "cpu_baseline" in o:
+                            line[other]["cpu_baseline"] = o["cpu_baseline"]
+                sub.steps = 30
                 b = run_batched(sub, CONFIGS["batched"], rank, world)
                 srv_cfg = dict(CONFIGS["serving"], arrivals_s=1.0)
                 sv = run_serving(sub, srv_cfg, rank, world)

@@ -16,6 +16,8 @@ LIB_PATH = os.path.join(_HERE, "libgtc_b200.so")
 
 # gtc_status values
 GTC_OK = 0
+GTC_ERR_INVALID_CSR = 2
+GTC_ERR_OUT_OF_MEMORY = 5
 STATUS_NAMES = {
     0: "GTC_OK", 1: "GTC_ERR_INVALID_ARGUMENT", 2: "GTC_ERR_INVALID_CSR",
     3: "GTC_ERR_WORKSPACE_TOO_SMALL", 4: "GTC_ERR_CUDA", 5: "GTC_ERR_OUT_OF_MEMORY",
@@ -34,6 +36,7 @@ _SIGNATURES = {
     "gtc_count_tuned": (c_int, [P, c_int, P, c_int64, c_int64, c_int, P, P, P, P, P, c_size_t, P,
                                 P]),
     "gtc_count_launches": (c_int, [c_int64, c_int64, c_int, P, P, P]),
+    "gtc_count_status": (c_int, [P, c_size_t, P, P]),
     "gtc_count_phase_times": (c_int, [P, c_int, P, c_int64, c_int64, P, c_size_t, P]),
     "gtc_count_noalloc": (c_int, [P, c_int, P, c_int64, c_int64, c_int, P, P, P, P, P]),
     "gtc_batch_workspace_size": (c_int, [c_int64, c_int64, c_int64, P]),

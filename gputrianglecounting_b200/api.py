@@ -57,6 +57,23 @@ def _check_csr_tensors(off: torch.Tensor, ind: torch.Tensor) -> int:
     return 32 if off.dtype == torch.int32 else 64
 
 
+def _alloc_workspace(nbytes: int, device) -> torch.Tensor:
+    """A device workspace of at least nbytes (256-byte aligned: torch's
+    caching allocator hands out 512-byte aligned blocks).  An allocation
+    failure surfaces as GTCError(GTC_ERR_OUT_OF_MEMORY); the caller keeps no
+    partial state."""
+    try:
+        return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+    except torch.cuda.OutOfMemoryError as e:
+        raise GTCError(_lib.GTC_ERR_OUT_OF_MEMORY, f"workspace of {nbytes} bytes") from e
+
+
+def _check_workspace_status(ws: torch.Tensor, stream) -> None:
+    bits = ctypes.c_uint32(0)
+    check(_lib.load().gtc_count_status(ws.data_ptr(), ws.numel(), _stream_handle(stream),
+                                       ctypes.byref(bits)), "gtc_count_status")
+
+
 @dataclass
 class TriangleCounts:
     """Outputs of one count (device tensors; scalars read on demand)."""
@@ -100,8 +117,20 @@ class TriangleCounter:
         if self._ws is None or self._ws.numel() < nbytes:
             self._ws = None
             # 256-byte alignment: torch's caching allocator returns 512-aligned blocks
-            self._ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+            self._ws = _alloc_workspace(nbytes, self.device)
         return self._ws
+
+    def release(self) -> None:
+        """Drop the cached workspace (it is re-allocated by the next count)."""
+        self._ws = None
+
+    def check_status(self, stream=None) -> None:
+        """Device-side error report of the last count on this counter (waits
+        for `stream`): raises GTCError(GTC_ERR_INVALID_CSR) if that count met
+        a neighbour id outside [0, n), which the kernels skip instead of
+        dereferencing."""
+        if self._ws is not None:
+            _check_workspace_status(self._ws, stream)
 
     def count(self, off: torch.Tensor, ind: torch.Tensor, mode: str = "plain",
               outputs=("r", "t", "lcc"), out: TriangleCounts | None = None,
@@ -260,6 +289,14 @@ class BatchCSR:
         return CSRGraph((off - e0).contiguous(), self.ind[e0:e1].contiguous(), f"g{g}")
 
 
+def batch_workspace_bytes(num_graphs: int, total_n: int, total_nnz: int) -> int:
+    """Device workspace of one gtc_count_batch call (host-only query)."""
+    out = ctypes.c_size_t(0)
+    check(_lib.load().gtc_batch_workspace_size(num_graphs, total_n, total_nnz,
+                                               ctypes.byref(out)), "gtc_batch_workspace_size")
+    return int(out.value)
+
+
 @dataclass
 class BatchCounts:
     r: torch.Tensor | None          # int64[N] over the concatenated vertex space
@@ -280,17 +317,26 @@ class BatchCounter:
         self._pack_staging: torch.Tensor | None = None
 
     def workspace_bytes(self, num_graphs: int, total_n: int, total_nnz: int) -> int:
-        out = ctypes.c_size_t(0)
-        check(_lib.load().gtc_batch_workspace_size(num_graphs, total_n, total_nnz,
-                                                   ctypes.byref(out)), "gtc_batch_workspace_size")
-        return int(out.value)
+        return batch_workspace_bytes(num_graphs, total_n, total_nnz)
 
     def reserve(self, num_graphs: int, total_n: int, total_nnz: int) -> None:
         """Allocate the workspace up front (e.g. before a CUDA-graph capture)."""
         need = self.workspace_bytes(num_graphs, total_n, total_nnz)
         if self._ws is None or self._ws.numel() < need:
             self._ws = None
-            self._ws = torch.empty(max(need, 256), dtype=torch.uint8, device=self.device)
+            self._ws = _alloc_workspace(need, self.device)
+
+    def release(self) -> None:
+        """Drop the cached workspace and pack buffers."""
+        self._ws = None
+        self._pack_scratch = None
+        self._pack_staging = None
+
+    def check_status(self, stream=None) -> None:
+        """As TriangleCounter.check_status, for the last batch counted here
+        (a local id outside its graph's [0, n_g) raises GTC_ERR_INVALID_CSR)."""
+        if self._ws is not None:
+            _check_workspace_status(self._ws, stream)
 
     def alloc_outputs(self, batch: BatchCSR, outputs=("r", "lcc", "graph_T")) -> BatchCounts:
         dev, n, G = self.device, batch.total_n, batch.num_graphs

@@ -249,11 +249,17 @@ gtc_status launch_subset(const OffT *off, const IndT *ind, const VtxT *vertex,
 
 // ================================================================== compat
 
+// int64 neighbour ids -> int32.  An id outside [0, nv) becomes -1, which the
+// counting kernels flag (kErrIndexRange) and skip, so a wide id can never
+// wrap into a valid-looking one.
 __global__ void narrow_kernel(const long long *__restrict__ in, int *__restrict__ out,
-                              long long count)
+                              long long count, long long nv)
 {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count) out[i] = (int)in[i];
+    if (i < count) {
+        const long long x = in[i];
+        out[i] = (x >= 0 && x < nv) ? (int)x : -1;
+    }
 }
 
 __global__ void narrow_out_kernel(const long long *__restrict__ in, int *__restrict__ out,
@@ -270,6 +276,15 @@ struct CompatCache {
 std::mutex g_compat_mu;
 CompatCache g_compat[64];
 thread_local gtc_status g_compat_status = GTC_OK;
+// Workspace of this thread's last kernelCall shim that launched a count
+// (its status word is read by gtc_compat_last_status), or null.
+thread_local const void *g_compat_ws = nullptr;
+
+// Device error bits -> status.
+gtc_status status_from_bits(unsigned int bits)
+{
+    return (bits & kErrIndexRange) ? GTC_ERR_INVALID_CSR : GTC_OK;
+}
 
 void *compat_workspace(size_t bytes)
 {
@@ -438,6 +453,7 @@ gtc_status gtc_validate_csr(const void *d_off, int off_bits, const int32_t *d_in
         return GTC_ERR_INVALID_ARGUMENT;
     if (off_bits != 32 && off_bits != 64) return GTC_ERR_INVALID_ARGUMENT;
     if (n > 0x7fffffffll) return GTC_ERR_UNSUPPORTED;
+    if (reinterpret_cast<uintptr_t>(d_workspace) & 255) return GTC_ERR_INVALID_ARGUMENT;
     if (ws_bytes < gtc_validate_workspace_size(n, nnz)) return GTC_ERR_WORKSPACE_TOO_SMALL;
     if (off_bits == 32)
         return run_validate<int>(static_cast<const int *>(d_off), d_ind, n, nnz, d_workspace,
@@ -462,7 +478,34 @@ gtc_status gtc_count_subset(const void *d_off, int off_bits, const int32_t *d_in
     return GTC_ERR_INVALID_ARGUMENT;
 }
 
-gtc_status gtc_compat_last_status(void) { return g_compat_status; }
+gtc_status gtc_compat_last_status(void)
+{
+    if (g_compat_status != GTC_OK || !g_compat_ws) return g_compat_status;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return GTC_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_compat_mu);
+    // the cached workspace was replaced by a later, larger call: its status
+    // word belonged to that call
+    if (g_compat[dev].ptr != g_compat_ws) return g_compat_status;
+    unsigned int bits = 0;
+    // a copy on the legacy default stream, so it waits for the count
+    if (cudaMemcpy(&bits, g_compat_ws, sizeof(bits), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return GTC_ERR_CUDA;
+    return status_from_bits(bits);
+}
+
+gtc_status gtc_count_status(const void *d_workspace, size_t ws_bytes, gtc_stream_t stream,
+                            uint32_t *h_bits)
+{
+    if (!d_workspace || ws_bytes < sizeof(unsigned int)) return GTC_ERR_INVALID_ARGUMENT;
+    unsigned int bits = 0;
+    cudaStream_t s = as_stream(stream);
+    if (cudaMemcpyAsync(&bits, d_workspace, sizeof(bits), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return GTC_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return GTC_ERR_CUDA;
+    if (h_bits) *h_bits = bits;
+    return status_from_bits(bits);
+}
 
 gtc_status gtc_compat_release(void)
 {
@@ -482,6 +525,7 @@ void gtc_kernelCall_i64(unsigned int numberBlocks, unsigned int numberThreads, i
 {
     (void)numberBlocks; (void)threads_per_block; (void)number_blocks; (void)shifter;
     g_compat_status = GTC_OK;
+    g_compat_ws = nullptr;
     if (!compat_block_size_ok(numberThreads)) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
     if (nv <= 0 || !d_off || !out) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
     int64_t nnz = 0;
@@ -498,11 +542,12 @@ void gtc_kernelCall_i64(unsigned int numberBlocks, unsigned int numberThreads, i
     int *ind32 = reinterpret_cast<int *>(ws + need);
     if (nnz > 0)
         narrow_kernel<<<(unsigned)div_up<long long>(nnz, 256), 256>>>(
-            reinterpret_cast<const long long *>(d_ind), ind32, nnz);
+            reinterpret_cast<const long long *>(d_ind), ind32, nnz, nv);
     RowConfig cfg = pick_row_config(nv, nnz);
     g_compat_status = run_count<long long>(reinterpret_cast<const long long *>(d_off), ind32, nv,
                                            nnz, true, reinterpret_cast<long long *>(out), nullptr,
                                            nullptr, nullptr, ws, need, 0, cfg, nullptr);
+    if (g_compat_status == GTC_OK) g_compat_ws = ws;
 }
 
 void gtc_kernelCall_i32(unsigned int numberBlocks, unsigned int numberThreads, int32_t nv,
@@ -511,6 +556,7 @@ void gtc_kernelCall_i32(unsigned int numberBlocks, unsigned int numberThreads, i
 {
     (void)numberBlocks; (void)threads_per_block; (void)number_blocks; (void)shifter;
     g_compat_status = GTC_OK;
+    g_compat_ws = nullptr;
     if (!compat_block_size_ok(numberThreads)) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
     if (nv <= 0 || !d_off || !out) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
     int32_t nnz = 0;
@@ -527,8 +573,10 @@ void gtc_kernelCall_i32(unsigned int numberBlocks, unsigned int numberThreads, i
     RowConfig cfg = pick_row_config(nv, nnz);
     g_compat_status = run_count<int>(d_off, d_ind, nv, nnz, true, r64, nullptr, nullptr, nullptr,
                                      ws, need, 0, cfg, nullptr);
-    if (g_compat_status == GTC_OK)
+    if (g_compat_status == GTC_OK) {
         narrow_out_kernel<<<(unsigned)div_up<long long>(nv, 256), 256>>>(r64, out, nv);
+        g_compat_ws = ws;
+    }
 }
 
 void gtc_kernelCall_vertex_i64(unsigned int numberBlocks, unsigned int numberThreads, int64_t nv,
@@ -538,6 +586,7 @@ void gtc_kernelCall_vertex_i64(unsigned int numberBlocks, unsigned int numberThr
 {
     (void)numberBlocks; (void)threads_per_block; (void)number_blocks; (void)shifter;
     g_compat_status = GTC_OK;
+    g_compat_ws = nullptr;
     if (!compat_block_size_ok(numberThreads)) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
     if (nv < 0 || (nv > 0 && (!vertex || !d_off || !d_ind || !out))) {
         g_compat_status = GTC_ERR_INVALID_ARGUMENT;
@@ -556,6 +605,7 @@ void gtc_kernelCall_vertex_i32(unsigned int numberBlocks, unsigned int numberThr
 {
     (void)numberBlocks; (void)threads_per_block; (void)number_blocks; (void)shifter;
     g_compat_status = GTC_OK;
+    g_compat_ws = nullptr;
     if (!compat_block_size_ok(numberThreads)) { g_compat_status = GTC_ERR_INVALID_ARGUMENT; return; }
     if (nv < 0 || (nv > 0 && (!vertex || !d_off || !d_ind || !out))) {
         g_compat_status = GTC_ERR_INVALID_ARGUMENT;

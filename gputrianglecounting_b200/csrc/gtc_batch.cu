@@ -45,7 +45,9 @@ __device__ __forceinline__ long long owner(const long long *__restrict__ start, 
 }
 
 // ind_g[e] = ind[e] + vstart[graph of e]; a block covers kChunk entries and
-// its threads walk forward from the block's first graph.
+// its threads walk forward from the block's first graph.  A local id outside
+// its graph's [0, n_g) becomes -1, which the counting kernels flag
+// (kErrIndexRange) and skip instead of crediting another graph's vertex.
 __global__ void globalize_kernel(const long long *__restrict__ estart,
                                  const long long *__restrict__ vstart, long long G,
                                  const int *__restrict__ ind, int *__restrict__ ind_g,
@@ -58,7 +60,9 @@ __global__ void globalize_kernel(const long long *__restrict__ estart,
     long long g = s_g0;
     for (long long e = e_begin + threadIdx.x; e < e_begin + kChunk && e < nnz; e += blockDim.x) {
         while (g + 1 < G && estart[g + 1] <= e) ++g;
-        ind_g[e] = ind[e] + (int)vstart[g];
+        const int x = ind[e];
+        const long long v0 = vstart[g];
+        ind_g[e] = (x >= 0 && x < vstart[g + 1] - v0) ? x + (int)v0 : -1;
     }
 }
 
@@ -130,14 +134,16 @@ struct BatchPlan {
 
 inline size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
+// The union graph's pipeline workspace comes first, so that the batch
+// workspace starts with its status word (gtc_count_status reads offset 0).
 BatchPlan make_batch_plan(long long G, long long total_n, long long total_nnz)
 {
     BatchPlan b;
     b.inner = make_plan(total_n, total_nnz, 64, true);
     size_t o = 0;
+    b.o_inner = o;  o = align256(o + b.inner.bytes);
     b.o_estart = o; o = align256(o + sizeof(long long) * (size_t)(G + 1));
     b.o_indg = o;   o = align256(o + sizeof(int) * (size_t)(total_nnz + 1));
-    b.o_inner = o;  o = align256(o + b.inner.bytes);
     b.bytes = o;
     return b;
 }

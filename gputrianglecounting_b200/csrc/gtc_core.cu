@@ -8,6 +8,7 @@
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
 #include <cooperative_groups/scan.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "gtc_core.cuh"
 
@@ -1251,6 +1252,15 @@ __global__ void global_kernel(const Counters *ctr, long long *global)
 
 namespace {
 
+// Host-side NVTX range around the launches of one pipeline phase (header-only
+// NVTX 3: a no-op unless a profiler injects itself).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
 int g_sm_count[64];
 int g_rows_blocks[64][8];
 int g_big_blocks[64][4];
@@ -1338,7 +1348,10 @@ gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
             return GTC_ERR_INVALID_ARGUMENT;
         cfg.group = tuning->group;
     }
+    // item_len and big_chunk bound the 16-bit shared hit counters: a counter
+    // collects at most one hit per adjacency entry of one work item
     if (tuning->item_len < 0 || (tuning->item_len > 0 && tuning->item_len < kMinItemLen) ||
+        tuning->item_len > kMaxItemLen ||
         tuning->big_chunk < 0 || tuning->big_hash_max < 0 ||
         tuning->big_hash_max > kBigHashMaxFdeg || tuning->big_chunk > 32768 ||
         tuning->labels < 0 || tuning->labels > 2 ||
@@ -1374,7 +1387,6 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
     unsigned int *status = reinterpret_cast<unsigned int *>(base + p.o_status);
     Counters *ctr = reinterpret_cast<Counters *>(base + p.o_counters);
     int *deg = reinterpret_cast<int *>(base + p.o_deg);
-    long long *tile = reinterpret_cast<long long *>(base + p.o_tile);
     void *scan_tmp = base + p.o_scan_tmp;
     int *fcnt = reinterpret_cast<int *>(base + p.o_fcnt);
     VInfo *vinfo = reinterpret_cast<VInfo *>(base + p.o_vinfo);
@@ -1388,6 +1400,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
     int *rank = reinterpret_cast<int *>(base + p.o_rank);
     int *order = reinterpret_cast<int *>(base + p.o_order);
 
+    NvtxRange count_range("gtc_count");
     int dev = 0;
     cudaGetDevice(&dev);
     cudaError_t err;
@@ -1401,6 +1414,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
     if (n > 0) {
         const unsigned vb = (unsigned)div_up<long long>(n, 256);
         if (timing) cudaEventRecord(timing->ev[0], stream);
+        nvtxRangePushA("gtc: forward lists");
         if (rank_labels) {
             const unsigned rb = (unsigned)div_up<long long>(n, kRankChunk);
             degree_hist_kernel<<<rb, kRankThreads, 0, stream>>>(off, off_bits, n, deg, hist);
@@ -1440,6 +1454,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
         vinfo_kernel<OffT><<<vb, 256, 0, stream>>>(off, fcnt, deg, rank_labels ? rank : nullptr, n,
                                                    small_cap, cfg.big_chunk, vinfo, big);
         err = exclusive_scan_i64(big, big, n, scan_tmp, stream);
+        nvtxRangePop();
         if (err != cudaSuccess) return GTC_ERR_CUDA;
         if (timing) cudaEventRecord(timing->ev[1], stream);
         const int *lorder = rank_labels ? order : nullptr;
@@ -1456,8 +1471,11 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                                                          status, irow, n_items, cfg.item_len,
                                                          small_cap, cfg.region_mult, lorder);
             };
-            if (per_vertex) launch_rows(count_rows_kernel<true, OffT>);
-            else launch_rows(count_rows_kernel<false, OffT>);
+            {
+                NvtxRange r("gtc: warp kernel");
+                if (per_vertex) launch_rows(count_rows_kernel<true, OffT>);
+                else launch_rows(count_rows_kernel<false, OffT>);
+            }
             if (timing) cudaEventRecord(timing->ev[2], stream);
             const size_t big_smem = sizeof(int) * kBigTableSlots +
                                     sizeof(unsigned int) * (kBigTableSlots / 2);
@@ -1469,6 +1487,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                                                                 cfg.big_hash_max, small_cap, lorder);
             };
             int *bc = g_big_blocks[dev & 63];
+            NvtxRange r("gtc: block kernel");
             if (rank_labels) {
                 if (per_vertex) launch_big(count_big_kernel<true, OffT, true>, &bc[3]);
                 else launch_big(count_big_kernel<false, OffT, true>, &bc[2]);

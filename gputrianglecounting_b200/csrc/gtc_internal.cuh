@@ -39,6 +39,7 @@ constexpr int kRowThreads = 256;            // warp-per-item count kernel
 constexpr int kRowSlots = 512;              // shared table slots per warp
 constexpr int kRowMinBlocks = 6;            // 48 warps per SM (register budget 42)
 constexpr int kMinItemLen = 32;             // smallest warp work item (entries)
+constexpr int kMaxItemLen = 65535;          // largest: a 16-bit hit counter must not carry
 constexpr int kBigThreads = 256;            // block-per-row count kernel (8 blocks/SM)
 constexpr int kBigTableLog2 = 12;
 constexpr int kBigTableSlots = 1 << kBigTableLog2;   // shared hash slots (block kernel)
@@ -61,10 +62,10 @@ constexpr int kTrimLoads = 4;               // block kernel: loads in flight per
 constexpr int kBitWords = 2048;             // block kernel rank bitmap: 65536 ranks
 constexpr int kBitKeys = 2048;              // longest apex list on the bitmap path
 
-// Error bits written to the workspace status word by device code.
+// Error bits written to the workspace status word (the first 4 bytes of
+// every counting workspace) by device code; gtc_count_status reads them.
 enum : unsigned int {
-    kErrIndexRange = 1u,   // a neighbour id outside [0, n) was met
-    kErrForwardOverflow = 2u,
+    kErrIndexRange = 1u,   // a neighbour id outside [0, n) was met (and skipped)
 };
 
 // Per-vertex record built once per count: forward-list start, forward degree

@@ -22,6 +22,9 @@
 //     them) race on it and must be serialised by the caller;
 //   * the first call on each device looks the array's device address up
 //     (cudaGetSymbolAddress); make that first call before any stream capture.
+//     The address is kept for the life of the process; a cudaDeviceReset
+//     makes it stale, so a process that resets a device must not use this
+//     entry point on that device afterwards.
 // The entry point calls no cudaMalloc, cudaFree or other allocating routine.
 #include <mutex>
 

@@ -86,13 +86,30 @@ gtc_status gtc_workspace_size(int64_t n, int64_t nnz, int off_bits,
  *   d_lcc       device double[n] or NULL (PLAIN mode only)
  *   d_global    device int64[3] or NULL: {T, 3T, 6T}
  *   d_workspace device, >= gtc_workspace_size bytes, 256-byte aligned
- * Asynchronous on `stream`; the caller synchronises.
+ * Asynchronous on `stream`; the caller synchronises.  The counting calls do
+ * not validate the input (like the reference's kernel), but a neighbour id
+ * outside [0, n) is never dereferenced: it is skipped and recorded in the
+ * workspace, and gtc_count_status then reports GTC_ERR_INVALID_CSR (the
+ * counts of such a graph are meaningless).
  */
 gtc_status gtc_count(const void *d_off, int off_bits, const int32_t *d_ind,
                      int64_t n, int64_t nnz, gtc_mode mode,
                      int64_t *d_r, int64_t *d_t, double *d_lcc,
                      int64_t *d_global, void *d_workspace, size_t ws_bytes,
                      gtc_stream_t stream);
+
+/*
+ * Device-side error report of the last count that used this workspace
+ * (gtc_count, gtc_count_tuned or gtc_count_batch; the status word is the
+ * workspace's first 4 bytes and each count clears it when it starts).
+ * Synchronous: waits for `stream`, then returns GTC_OK, or
+ * GTC_ERR_INVALID_CSR if a neighbour id outside its graph's vertex range was
+ * met.  h_bits (nullable) receives the raw error bits.  The reference has no
+ * counterpart: its launches are unchecked (include/clusteringCount.cuh:4-11,
+ * src/clusteringCount.cu:410-412).
+ */
+gtc_status gtc_count_status(const void *d_workspace, size_t ws_bytes,
+                            gtc_stream_t stream, uint32_t *h_bits);
 
 /*
  * Launch-shape overrides for gtc_count_tuned (0 in any field = the library's
@@ -102,7 +119,7 @@ gtc_status gtc_count(const void *d_off, int off_bits, const int32_t *d_ind,
  *   group        lanes that share one apex row in the group kernel: 4, 8,
  *                16 or 32; rows whose forward list is longer than
  *                4*group go to the block kernel
- *   item_len     adjacency entries per warp work item (>= 32)
+ *   item_len     adjacency entries per warp work item (32 .. 65535)
  *   big_chunk    adjacency entries per block-kernel work item (<= 32768)
  *   big_hash_max longest forward list the block kernel hashes in shared
  *                memory (<= 2048); longer lists are binary-searched in place
@@ -164,7 +181,10 @@ gtc_status gtc_count_phase_times(const void *d_off, int off_bits,
  * library holds the array until exit.  All calls on a device share it, so
  * calls that overlap on the GPU race and must be serialised.  The first call
  * on each device looks up the array's address; make it before any stream
- * capture.  Arguments and outputs as gtc_count; asynchronous on `stream`.
+ * capture.  The looked-up address is kept for the life of the process: after
+ * a cudaDeviceReset on that device it is stale, so a process that resets a
+ * device must not call this entry point on it again.  Arguments and outputs
+ * as gtc_count; asynchronous on `stream`.
  */
 gtc_status gtc_count_noalloc(const void *d_off, int off_bits,
                              const int32_t *d_ind, int64_t n, int64_t nnz,
@@ -226,7 +246,7 @@ gtc_status gtc_batch_pack(int64_t num_graphs, const void *const *h_off,
  * Check the CSR input contract on the device.  Synchronous: writes a
  * gtc_csr_reason to *h_reason and returns GTC_OK (the status reports only
  * call failures; an invalid graph is reported through *h_reason).
- * Workspace: gtc_validate_workspace_size(n, nnz) bytes.
+ * Workspace: gtc_validate_workspace_size(n, nnz) bytes, 256-byte aligned.
  */
 size_t gtc_validate_workspace_size(int64_t n, int64_t nnz);
 gtc_status gtc_validate_csr(const void *d_off, int off_bits,
@@ -271,7 +291,12 @@ void gtc_kernelCall_vertex_i32(unsigned int numberBlocks,
                                const int32_t *d_ind, int32_t *outPutTriangles,
                                int32_t threads_per_block,
                                int32_t number_blocks, int32_t shifter);
-/* Status of this host thread's last kernelCall shim call. */
+/* Status of this host thread's last kernelCall shim call: the host-side
+   outcome, and -- when that call launched a count -- the device error word of
+   that count, read after a copy on the legacy default stream (so this call
+   waits for the count; GTC_ERR_INVALID_CSR when a neighbour id was outside
+   [0, nv)).  Like the reference, the shims are not re-entrant across host
+   threads on one device: they share one cached workspace. */
 gtc_status gtc_compat_last_status(void);
 /* Releases the compat layer's cached workspace on the current device. */
 gtc_status gtc_compat_release(void);

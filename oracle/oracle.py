@@ -64,6 +64,8 @@ def ref_cpu_lib() -> ctypes.CDLL:
         "ref_cpu_tri_ne_i64": (c_int64, [c_int64, P, P, P]),
         "ref_cpu_tri_ne_i32": (c_int64, [ctypes.c_int32, P, P, P]),
         "ref_cpu_rows_omp_i64": (c_int64, [c_int64, P, P, P, c_int64, P, P, c_int]),
+        "ref_cpu_units_timed_i32": (c_int64, [ctypes.c_int32, P, P, P, P, P, c_int64, P, P, P,
+                                              c_int]),
         "ref_cpu_max_threads": (c_int, []),
     })
 
@@ -180,6 +182,43 @@ def ref_rows_prepared(off64, ind64, vertices64, tri, r, threads: int = 0) -> int
         None if vertices64 is None else vertices64.ctypes.data_as(c_void_p),
         off64.shape[0] - 1 if vertices64 is None else vertices64.shape[0],
         tri.ctypes.data_as(c_void_p), r.ctypes.data_as(c_void_p), threads))
+
+
+def ref_units_timed(off32, ind32, unit_rows, unit_off, units, threads: int = 0,
+                    tri=None, r=None):
+    """The reference's vertex-list count (int32 CSR) over the listed units of
+    rows (unit u = unit_rows[unit_off[u]:unit_off[u+1]]), one unit per
+    OpenMP task.  Returns (unit_ns int64[len(units)], total of triNE over the
+    rows run).  tri and r (int64[nnz], int64[n]) may be passed preallocated;
+    r[v] receives each run row's sum of triNE."""
+    off32 = np.ascontiguousarray(off32, np.int32)
+    ind32 = np.ascontiguousarray(ind32, np.int32)
+    unit_rows = np.ascontiguousarray(unit_rows, np.int64)
+    unit_off = np.ascontiguousarray(unit_off, np.int64)
+    units = np.ascontiguousarray(units, np.int64)
+    if tri is None:
+        tri = np.zeros(ind32.shape[0], np.int64)
+    if r is None:
+        r = np.zeros(off32.shape[0] - 1, np.int64)
+    ns = np.zeros(units.shape[0], np.int64)
+    P = lambda a: a.ctypes.data_as(c_void_p)  # noqa: E731
+    total = ref_cpu_lib().ref_cpu_units_timed_i32(
+        off32.shape[0] - 1, P(off32), P(ind32), P(unit_rows), P(unit_off), P(units),
+        units.shape[0], P(tri), P(r), P(ns), threads)
+    return ns, int(total)
+
+
+def ref_all_rows_i32(off32, ind32, threads: int = 0, chunk: int = 64):
+    """r for every row through the timed form (units of `chunk` consecutive
+    rows); returns (r, total)."""
+    n = off32.shape[0] - 1
+    rows = np.arange(n, dtype=np.int64)
+    uoff = np.minimum(np.arange(0, n + chunk, chunk, dtype=np.int64), n)
+    uoff = np.unique(uoff)
+    r = np.zeros(n, np.int64)
+    _, total = ref_units_timed(off32, ind32, rows, uoff, np.arange(uoff.shape[0] - 1), threads,
+                               r=r)
+    return r, total
 
 
 def max_threads() -> int:

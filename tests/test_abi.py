@@ -88,6 +88,22 @@ def test_invalid_arguments_rejected_before_any_device_work():
     bad = _lib.Tuning(labels=5)
     assert lib.gtc_count_tuned(fake, 32, fake, 10, 4, 0, None, None, None, None, fake, 1 << 20,
                                None, ctypes.byref(bad)) == 1
+    # item_len above 65535 could carry a 16-bit shared hit counter into its
+    # neighbour; rejected (host-only check, also in the launch plan)
+    bad = _lib.Tuning(item_len=65536)
+    assert lib.gtc_count_tuned(fake, 32, fake, 10, 4, 0, None, None, None, None, fake, 1 << 20,
+                               None, ctypes.byref(bad)) == 1
+    from gputrianglecounting_b200 import api
+    assert api.launch_plan(1000, 90000, tuning={"item_len": 65535})["launches"] > 0
+    with pytest.raises(_lib.GTCError):
+        api.launch_plan(1000, 90000, tuning={"item_len": 65536})
+    # status query needs a workspace
+    assert lib.gtc_count_status(None, 256, None, None) == 1
+    assert lib.gtc_count_status(fake, 2, None, None) == 1
+    # validator: misaligned workspace
+    reason = ctypes.c_int32(-1)
+    assert lib.gtc_validate_csr(fake, 32, fake, 10, 4, ctypes.c_void_p(264), 1 << 10,
+                                ctypes.byref(reason), None) == 1
     assert lib.gtc_count_subset(None, 32, None, None, -1, None, None) == 1
     assert lib.gtc_count_subset(None, 32, None, None, 0, None, None) == 0
 

@@ -102,3 +102,47 @@ def test_batched_workload_sample(cuda):
     res = api.BatchCounter(cuda).count(batch)
     torch.cuda.synchronize()
     _check_against_oracle([g.numpy() for g in graphs], batch, res)
+
+
+def test_batch_local_id_out_of_range_is_reported(cuda):
+    """A graph-local id outside its graph's [0, n_g) is turned into an
+    out-of-range id (never another graph's vertex) and reported."""
+    graphs = _mixed_graphs()[:8]
+    batch = G.concat_graphs(graphs, cuda)
+    bc = api.BatchCounter(cuda)
+    bc.count(batch)
+    bc.check_status()
+    bad = batch.ind.clone()
+    v0 = int(batch.vstart[3])
+    n3 = int(batch.vstart[4]) - v0
+    bad[int(batch.off[v0]) + 1] = n3          # valid id in graph 4, not in graph 3
+    bc.count(api.BatchCSR(batch.vstart, batch.off, bad))
+    with pytest.raises(api.GTCError) as e:
+        bc.check_status()
+    assert e.value.status == 2
+
+
+def test_full_batched_workload_per_vertex_equals_single_graph(cuda):
+    """All 4,096 graphs of the batched workload: every per-vertex r and lcc
+    of the one-launch batch equals the graph counted alone by gtc_count, and
+    every per-graph T matches (the first 48 graphs are also checked against
+    the oracle in test_batched_workload_sample)."""
+    specs = G.batched_specs(4096, 4)
+    graphs = [G.make_spec_graph(s, cuda) for s in specs]
+    batch = G.concat_graphs(graphs, cuda)
+    bc = api.BatchCounter(cuda)
+    res = bc.count(batch, outputs=("r", "lcc", "graph_T"))
+    bc.check_status()
+    tc = api.TriangleCounter(cuda)
+    r_one = torch.empty_like(res.r)
+    lcc_one = torch.empty_like(res.lcc)
+    T_one = torch.empty(len(graphs), 3, dtype=torch.int64, device=cuda)
+    vstart = batch.vstart.cpu().numpy()
+    for i, g in enumerate(graphs):
+        sl = slice(int(vstart[i]), int(vstart[i + 1]))
+        tc.count(g.off, g.ind, out=api.TriangleCounts(r=r_one[sl], t=None, lcc=lcc_one[sl],
+                                                      global_counts=T_one[i]))
+    torch.cuda.synchronize()
+    assert torch.equal(res.r, r_one)
+    assert torch.equal(res.lcc.view(torch.int64), lcc_one.view(torch.int64))
+    assert torch.equal(res.graph_T, T_one[:, 0])

@@ -45,3 +45,29 @@ def test_launch_counts_follow_the_library_plan():
         per = bench.launches_per_count(n, nnz, {"labels": lab})
         assert per == (13 if lab == 1 else 15)
         assert bench.batch_launches(n, nnz, {"labels": lab}) == per + 2
+
+
+def test_reference_timer_units_and_sampling():
+    """The reference arm's timer: its units cover every row exactly once, a
+    whole-graph step reproduces the reference's per-vertex r, and the k
+    phases of the systematic light-unit sample cover every light unit
+    exactly once (so the per-step estimates average to the full graph)."""
+    from oracle import oracle as O
+    g = bench.int32_offsets(G.rmat(11, 16, 3).numpy())
+    rt = bench.ReferenceTimer(g, threads=2, step_s=1e-9)
+    rows = np.sort(rt.unit_rows)
+    assert np.array_equal(rows, np.arange(g.n))
+    assert rt.unit_off[0] == 0 and rt.unit_off[-1] == g.n
+    assert rt.n_heavy > 0                      # the hubs of an R-MAT graph
+    rt.calibrate()
+    assert not rt.whole and rt.k >= 1
+    seen = np.concatenate([rt.light_units[p::rt.k] for p in range(rt.k)])
+    assert np.array_equal(np.sort(seen), np.arange(rt.n_heavy, rt.unit_off.shape[0] - 1))
+    st = rt.step(0)
+    assert st["full_s"] > 0 and st["wall_s"] > 0
+    whole = bench.ReferenceTimer(g, threads=2, step_s=1e9)
+    whole.calibrate()
+    assert whole.whole
+    whole.step(0)
+    r_ref, _, _, _ = O.per_vertex(g.off, g.ind)
+    assert np.array_equal(whole.r, r_ref)

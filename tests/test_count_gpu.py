@@ -243,29 +243,51 @@ def test_reference_gpu_kernel_parity(cuda):
         assert torch.equal(res.r, ref_out)
 
 
-@pytest.mark.parametrize("which", ["rmat20", "rgg4m"])
-def test_full_size_properties(cuda, which):
-    """Full-size configs: size-independent properties (the oracle would take
-    minutes): plain and oriented modes agree, sum t = 3T, r even,
-    t <= C(d, 2), lcc in [0, 1], repeat runs identical, and a seeded row
-    sample matches the oracle's per-row count exactly."""
-    g = (G.rmat(20, 16, 2) if which == "rmat20" else G.rgg2d(1 << 22, 12, 3)).to(cuda)
+def test_out_of_range_ids_are_reported_not_dereferenced(cuda):
+    """A neighbour id outside [0, n) is never dereferenced: the kernels skip
+    it and gtc_count_status reports GTC_ERR_INVALID_CSR.  The bad ids sit in
+    the largest row (a block-kernel apex) and in a low-degree row (warp
+    kernel), under both labelings; a valid count on the same workspace then
+    reports OK again (each count clears the status word)."""
+    g = G.rmat(12, 16, 3).numpy()
     counter = api.TriangleCounter(cuda)
-    a = counter.count(g.off, g.ind)
-    b = counter.count(g.off, g.ind, mode="oriented")
+    d_off, d_ind = _dev(g.off, g.ind, cuda)
+    counter.count(d_off, d_ind)
+    counter.check_status()
+    deg = np.diff(g.off)
+    hub = int(np.argmax(deg))
+    low = int(np.argmin(np.where(deg >= 2, deg, 1 << 30)))
+    for bad in (g.n, g.n + 12345, -1, -(1 << 31), (1 << 31) - 1):
+        ind = g.ind.copy()
+        ind[g.off[hub] + deg[hub] // 2] = bad
+        ind[g.off[low] + 1] = bad
+        bad_ind = torch.from_numpy(ind).to(cuda)
+        for tun in (None, {"labels": 1}, {"labels": 2}, {"group": 4, "big_hash_max": 8}):
+            counter.count(d_off, bad_ind, tuning=tun)
+            with pytest.raises(api.GTCError) as e:
+                counter.check_status()
+            assert e.value.status == 2
+        counter.count(d_off, bad_ind, mode="oriented")
+        with pytest.raises(api.GTCError):
+            counter.check_status()
+    res = counter.count(d_off, d_ind)
+    counter.check_status()
+    _check(g.off, g.ind, res)
+
+
+def test_compat_wide_id_is_reported(cuda):
+    """kernelCall<int64_t> with an id that does not fit the graph (2^32 + 3
+    would wrap to 3 if narrowed blindly) reports GTC_ERR_INVALID_CSR through
+    gtc_compat_last_status instead of counting a wrapped id."""
+    g = G.wheel(30).numpy()
+    off = torch.from_numpy(g.off).to(cuda)
+    ind = torch.from_numpy(g.ind.astype(np.int64)).to(cuda)
+    out = torch.zeros(g.n, dtype=torch.int64, device=cuda)
+    api.kernelCall(1, 256, g.n, off, ind, out, 1, 256, 0)
     torch.cuda.synchronize()
-    T = a.triangles
-    assert b.triangles == T
-    assert int(a.t.sum().item()) == 3 * T
-    assert int((a.r % 2).sum().item()) == 0
-    deg = (g.off[1:] - g.off[:-1])
-    assert bool((a.t <= deg * (deg - 1) // 2).all())
-    assert bool(((a.lcc >= 0) & (a.lcc <= 1)).all())
-    c = counter.count(g.off, g.ind)
-    torch.cuda.synchronize()
-    assert torch.equal(a.r, c.r)
-    rng = np.random.default_rng(11)
-    rows = rng.integers(0, g.n, 300).astype(np.int32)
-    h = g.numpy()
-    sub = O.subset(h.off, h.ind, rows)
-    assert np.array_equal(a.r.cpu().numpy()[rows], sub)
+    r_ref, _, _, _ = O.per_vertex(g.off, g.ind)
+    assert np.array_equal(out.cpu().numpy(), r_ref)
+    ind[4] = (1 << 32) + 3
+    with pytest.raises(api.GTCError) as e:
+        api.kernelCall(1, 256, g.n, off, ind, out, 1, 256, 0)
+    assert e.value.status == 2
