@@ -637,7 +637,7 @@ __device__ __forceinline__ int sorted_find(const int *__restrict__ list,
 // that batch gives it.
 //   lookup(w) -> slot >= 0 on a hit, -1 on a miss (called with w > ka when TRIM)
 //   on_hit(slot, w): credit of the third vertex
-// Returns this lane's hit count (the apex credit).
+// Returns this lane's hit count (the apex credit).  G = 32: a whole warp.
 template <int G, bool PER_VERTEX, bool TRIM, typename Grp, class Lookup, class OnHit>
 __device__ __forceinline__ unsigned int
 probe_stride(const Grp &grp, long long s, long long end, int a, int ka, int fa, int cap,
@@ -676,26 +676,47 @@ probe_stride(const Grp &grp, long long s, long long end, int a, int ka, int fa, 
         const int px = grp.shfl(x, src);
         unsigned int hx = 0;
         if (TRIM) {
-            // windows of kTrimLoads * G elements from the end, all loads of a
-            // window in flight together
-            for (int top = len; top > 0; top -= kTrimLoads * G) {
-                int w[kTrimLoads];
+            // The members ranked above the apex are a suffix of the sorted
+            // list.  One sampled load finds how many whole G-element chunks,
+            // counted from the end, lie above ka (lane k reads the first
+            // element of chunk k); those are swept without a per-element
+            // test, kTrimLoads chunks in flight, and only the chunk that
+            // holds the cut is masked.
+            int top = len;
+            while (top > 0) {
+                const int js = top - G * (lane + 1);
+                const int smp = js >= 0 ? list[js] : ka;
+                const int nfull = __popc(grp.ballot(smp > ka));
+                const int stop = top - G * nfull;
+                for (int base = top; base > stop; base -= kTrimLoads * G) {
+                    int w[kTrimLoads];
 #pragma unroll
-                for (int u = 0; u < kTrimLoads; ++u) {
-                    const int j = top - (u + 1) * G + lane;
-                    w[u] = j >= 0 ? list[j] : ka;
-                }
+                    for (int u = 0; u < kTrimLoads; ++u) {
+                        const int j = base - (u + 1) * G + lane;
+                        w[u] = j >= stop ? list[j] : -1;      // ranks are >= 0
+                    }
 #pragma unroll
-                for (int u = 0; u < kTrimLoads; ++u) {
-                    const int sl = w[u] > ka ? lookup(w[u]) : -1;
-                    if (sl >= 0) {
-                        ++hx;
-                        if (PER_VERTEX) on_hit(sl, w[u]);
+                    for (int u = 0; u < kTrimLoads; ++u) {
+                        if (w[u] >= 0) {
+                            const int sl = lookup(w[u]);
+                            if (sl >= 0) {
+                                ++hx;
+                                if (PER_VERTEX) on_hit(sl, w[u]);
+                            }
+                        }
                     }
                 }
-                // sorted: once a loaded element is at or below ka, so is
-                // every element before it (lanes past the list start load ka)
-                if (grp.any(w[kTrimLoads - 1] <= ka)) break;
+                top = stop;
+                if (nfull < G) break;
+            }
+            if (top > 0) {                       // the chunk holding the cut
+                const int j = top - G + lane;
+                const int w0 = j >= 0 ? list[j] : ka;
+                const int sl = w0 > ka ? lookup(w0) : -1;
+                if (sl >= 0) {
+                    ++hx;
+                    if (PER_VERTEX) on_hit(sl, w0);
+                }
             }
         } else {
             int j = lane;
@@ -723,7 +744,7 @@ probe_stride(const Grp &grp, long long s, long long end, int a, int ka, int fa, 
             }
         }
         if (PER_VERTEX) {
-            const unsigned int hs = cg::reduce(grp, hx, cg::plus<unsigned int>());
+            const unsigned int hs = __reduce_add_sync(0xffffffffu, hx);
             if (lane == 0 && hs) atomicAdd(&tacc[px], (unsigned long long)hs);
         }
         hits += hx;
@@ -792,15 +813,22 @@ __device__ __forceinline__ void flush_hits(const ApexTable &tab, int tsize, int 
     }
 }
 
-// First row of every warp work item (item k covers entries
-// [k*item_len, (k+1)*item_len)), all items at once, so no warp starts an item
-// with a dependent binary search.
+// Work-item tables, so that no warp or block starts an item with a dependent
+// binary search: the first row of every warp work item (item k covers
+// entries [k*item_len, (k+1)*item_len)), and the (row, chunk) of every
+// block-kernel item (vertex v owns items big[v] .. big[v+1]-1, big being the
+// exclusive scan of its chunk counts).
 template <typename OffT>
 __global__ void item_rows_kernel(const OffT *__restrict__ off, long long n, long long item_len,
-                                 long long n_items, long long *__restrict__ irow)
+                                 long long n_items, long long *__restrict__ irow,
+                                 const long long *__restrict__ big, int2 *__restrict__ bitem)
 {
     long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n_items) irow[k] = row_of_entry(off, n, k * item_len);
+    if (k < n) {
+        const long long b0 = big[k], b1 = big[k + 1];
+        for (long long c = b0; c < b1; ++c) bitem[c] = make_int2((int)k, (int)(c - b0));
+    }
 }
 
 // Shuffle co-rank: the lane i whose [incl_i - w_i, incl_i) holds f (incl is
@@ -1051,8 +1079,8 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                  const int *__restrict__ find,
                  unsigned long long *__restrict__ tacc, Counters *ctr,
                  unsigned int *status, const long long *__restrict__ big_pre,
-                 int big_chunk, int big_hash_max, int small_cap,
-                 const int *__restrict__ order)
+                 const int2 *__restrict__ bitem, int big_chunk, int big_hash_max,
+                 int small_cap, const int *__restrict__ order)
 {
     extern __shared__ int smem[];
     int *keys = smem;
@@ -1076,8 +1104,9 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
         __syncthreads();
         const long long item = s_item;
         if (item >= n_items) break;
-        const long long a = row_of_entry(big_pre, n, item);
-        const long long chunk = item - big_pre[a];
+        const int2 it = bitem[item];
+        const long long a = it.x;
+        const long long chunk = it.y;
         const long long rb = (long long)off[a] + chunk * big_chunk;
         long long re = rb + big_chunk;
         if (re > (long long)off[a + 1]) re = off[a + 1];
@@ -1319,6 +1348,8 @@ Plan make_plan(long long n, long long nnz, int off_bits, bool per_vertex)
     p.o_big = take(sizeof(long long) * (size_t)(n + 1));
     p.o_trow = take(sizeof(long long) * (size_t)(p.n_tiles + 1));
     p.o_irow = take(sizeof(long long) * (size_t)(div_up<long long>(nnz, kMinItemLen) + 1));
+    // block-kernel items: at most one per row plus one per kMinBigChunk entries
+    p.o_bitem = take(sizeof(int2) * (size_t)(n + div_up<long long>(nnz, kMinBigChunk) + 1));
     p.bytes = o;
     return p;
 }
@@ -1352,7 +1383,8 @@ gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
     // collects at most one hit per adjacency entry of one work item
     if (tuning->item_len < 0 || (tuning->item_len > 0 && tuning->item_len < kMinItemLen) ||
         tuning->item_len > kMaxItemLen ||
-        tuning->big_chunk < 0 || tuning->big_hash_max < 0 ||
+        tuning->big_chunk < 0 || (tuning->big_chunk > 0 && tuning->big_chunk < kMinBigChunk) ||
+        tuning->big_hash_max < 0 ||
         tuning->big_hash_max > kBigHashMaxFdeg || tuning->big_chunk > 32768 ||
         tuning->labels < 0 || tuning->labels > 2 ||
         (tuning->region != 0 && tuning->region != 2 && tuning->region != 4))
@@ -1395,6 +1427,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
     long long *big = reinterpret_cast<long long *>(base + p.o_big);
     long long *trow = reinterpret_cast<long long *>(base + p.o_trow);
     long long *irow = reinterpret_cast<long long *>(base + p.o_irow);
+    int2 *bitem = reinterpret_cast<int2 *>(base + p.o_bitem);
     const bool rank_labels = cfg.rank_labels;
     unsigned long long *hist = reinterpret_cast<unsigned long long *>(base + p.o_hist);
     int *rank = reinterpret_cast<int *>(base + p.o_rank);
@@ -1460,8 +1493,9 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
         const int *lorder = rank_labels ? order : nullptr;
         if (nnz > 0) {
             const long long n_items = div_up<long long>(nnz, cfg.item_len);
-            item_rows_kernel<OffT><<<(unsigned)div_up<long long>(n_items, 256), 256, 0, stream>>>(
-                off, n, cfg.item_len, n_items, irow);
+            const long long it_threads = n_items > n ? n_items : n;
+            item_rows_kernel<OffT><<<(unsigned)div_up<long long>(it_threads, 256), 256, 0,
+                                     stream>>>(off, n, cfg.item_len, n_items, irow, big, bitem);
             auto launch_rows = [&](auto kern) {
                 int blocks = occupancy_blocks(kern, kRowThreads, 0, dev,
                                               &g_rows_blocks[dev & 63][per_vertex ? 1 : 0]);
@@ -1483,7 +1517,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                 cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem);
                 int blocks = occupancy_blocks(kern, kBigThreads, big_smem, dev, cache);
                 kern<<<blocks, kBigThreads, big_smem, stream>>>(off, ind, n, vinfo, find, tacc, ctr,
-                                                                status, big, cfg.big_chunk,
+                                                                status, big, bitem, cfg.big_chunk,
                                                                 cfg.big_hash_max, small_cap, lorder);
             };
             int *bc = g_big_blocks[dev & 63];

@@ -41,6 +41,7 @@ constexpr int kRowMinBlocks = 6;            // 48 warps per SM (register budget 
 constexpr int kMinItemLen = 32;             // smallest warp work item (entries)
 constexpr int kMaxItemLen = 65535;          // largest: a 16-bit hit counter must not carry
 constexpr int kBigThreads = 256;            // block-per-row count kernel (8 blocks/SM)
+constexpr int kMinBigChunk = 32;            // smallest block-kernel item (entries)
 constexpr int kBigTableLog2 = 12;
 constexpr int kBigTableSlots = 1 << kBigTableLog2;   // shared hash slots (block kernel)
 constexpr int kBigHashMaxFdeg = 2048;       // longest list hashed (load <= 1/2)
@@ -126,7 +127,8 @@ struct Plan {
     // workspace byte offsets
     size_t o_status = 0, o_counters = 0, o_deg = 0, o_tile = 0, o_scan_tmp = 0,
            o_fcnt = 0, o_vinfo = 0, o_find = 0, o_tacc = 0, o_big = 0,
-           o_bigpre = 0, o_trow = 0, o_irow = 0, o_hist = 0, o_rank = 0, o_order = 0;
+           o_bigpre = 0, o_trow = 0, o_irow = 0, o_hist = 0, o_rank = 0, o_order = 0,
+           o_bitem = 0;
     size_t bytes = 0;
 };
 

@@ -120,7 +120,7 @@ gtc_status gtc_count_status(const void *d_workspace, size_t ws_bytes,
  *                16 or 32; rows whose forward list is longer than
  *                4*group go to the block kernel
  *   item_len     adjacency entries per warp work item (32 .. 65535)
- *   big_chunk    adjacency entries per block-kernel work item (<= 32768)
+ *   big_chunk    adjacency entries per block-kernel work item (32 .. 32768)
  *   big_hash_max longest forward list the block kernel hashes in shared
  *                memory (<= 2048); longer lists are binary-searched in place
  *   labels       how forward lists name vertices: 1 = vertex ids (order by
