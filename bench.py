@@ -501,7 +501,7 @@ def run_b200(args, name: str, rank: int, world: int, with_baseline: bool = True)
 
 def launches_per_count(n: int, nnz: int, tuning: dict | None = None) -> int:
     """Kernels of one plain count with every output (the library's own plan:
-    13 with vertex-id labels, 15 with degree-rank labels)."""
+    5 with vertex-id labels, 11 with degree-rank labels)."""
     from gputrianglecounting_b200 import api
     return api.launch_plan(n, nnz, tuning=tuning)["launches"]
 

@@ -9,6 +9,7 @@
 #include <cooperative_groups/reduce.h>
 #include <cooperative_groups/scan.h>
 #include <nvtx3/nvToolsExt.h>
+#include <type_traits>
 
 #include "gtc_core.cuh"
 
@@ -21,20 +22,6 @@ namespace gtc {
 __device__ __forceinline__ int rank_bucket(int d)
 {
     return d < 0 ? 0 : (d < kRankBuckets ? d : kRankBuckets - 1);
-}
-
-__global__ void degree_kernel(const void *off_v, int off_bits, long long n,
-                              int *__restrict__ deg)
-{
-    long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    if (off_bits == 32) {
-        const int *off = static_cast<const int *>(off_v);
-        deg[v] = off[v + 1] - off[v];
-    } else {
-        const long long *off = static_cast<const long long *>(off_v);
-        deg[v] = (int)(off[v + 1] - off[v]);
-    }
 }
 
 // Degree of vertex v (0 past the end).
@@ -461,7 +448,8 @@ __device__ void warp_sort_global(int *list, int len, int lane)
     }
 }
 
-// One list of len >= 2 sorted by the whole warp.
+// One list of len >= 2 sorted by the whole warp: in registers up to
+// kSortRegMax, in place in global memory beyond.
 __device__ __forceinline__ void warp_sort_list(int *list, int len, int lane)
 {
     if (len <= 32) warp_sort_regs<1>(list, len, lane);
@@ -479,10 +467,9 @@ __device__ __forceinline__ void warp_sort_list(int *list, int len, int lane)
 // the long partners' (32 or more); shorter lists are only ever read whole (as
 // warp-kernel apexes, whose tables do not care about order, or as short
 // partners, whose members are each checked against the apex rank).
-// One warp per 32 consecutive rows, one list at a time: in registers up to
-// kSortRegMax elements, in place beyond.  Groups come from a dynamic queue,
-// so the few groups holding several long lists do not set the kernel's
-// length.
+// One warp per 32 consecutive rows, one list at a time (warp_sort_list).
+// Groups come from a dynamic queue, so the few groups holding several long
+// lists do not set the kernel's length.
 template <typename OffT>
 __global__ void __launch_bounds__(kSortThreads, 4)
 sort_lists_kernel(const OffT *__restrict__ off, const int *__restrict__ fcnt, long long n,
@@ -510,36 +497,35 @@ sort_lists_kernel(const OffT *__restrict__ off, const int *__restrict__ fcnt, lo
     }
 }
 
-// Vertex-id labels: restore id order in the rows whose forward entries the
-// placement split between tiles (all other rows keep the order of their
-// sorted CSR row).  One warp per tile boundary; a row holding several
-// boundaries is sorted once, by the warp of the first boundary inside it.
+// Work items of the two count kernels, written by the row that owns them so
+// that neither kernel starts an item with a search:
+//   * block-kernel items: a row whose forward list exceeds the warp kernel's
+//     table gets ceil(deg / big_chunk) items (row, chunk), at positions taken
+//     from one atomic counter (their order does not matter);
+//   * warp-kernel items: item k covers entries [k*item_len, (k+1)*item_len);
+//     the row holding entry k*item_len records itself as the item's first row.
 template <typename OffT>
-__global__ void __launch_bounds__(kSortThreads, 4)
-sort_split_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ fcnt,
-                       const long long *__restrict__ trow, long long n_tiles, long long n,
-                       int *__restrict__ find)
+__device__ __forceinline__ void post_row_items(long long v, long long b, long long e, int d,
+                                               int fdeg, int small_cap, int big_chunk,
+                                               long long item_len, Counters *ctr,
+                                               int2 *__restrict__ bitem,
+                                               long long *__restrict__ irow)
 {
-    const int lane = threadIdx.x & 31;
-    const long long t = (long long)blockIdx.x * (kSortThreads / 32) + (threadIdx.x >> 5) + 1;
-    if (t >= n_tiles) return;
-    const long long r = trow[t];
-    if (r >= n) return;
-    const long long beg = (long long)off[r];
-    if (!(beg < t * kPrepTile - r)) return;                  // boundary not inside row r
-    if (t > 1 && trow[t - 1] == r && beg < (t - 1) * kPrepTile - r) return;
-    const int len = fcnt[r];
-    if (len >= 2) warp_sort_list(find + beg, len, lane);
+    if (fdeg > small_cap) {
+        const int k = (int)div_up<long long>(d, big_chunk);
+        const unsigned long long at = atomicAdd(&ctr->big_total, (unsigned long long)k);
+        for (int c = 0; c < k; ++c) bitem[at + c] = make_int2((int)v, c);
+    }
+    for (long long k = div_up<long long>(b, item_len); k * item_len < e; ++k) irow[k] = v;
 }
 
-// Per-vertex record and block-kernel work: rows whose forward list exceeds
-// the group kernel's table get ceil(deg / big_chunk) block items.
+// Rank labels: per-vertex record and work items (one thread per vertex).
 template <typename OffT>
 __global__ void vinfo_kernel(const OffT *__restrict__ off, const int *__restrict__ fcnt,
                              const int *__restrict__ deg, const int *__restrict__ rank,
-                             long long n, int small_cap, int big_chunk,
-                             VInfo *__restrict__ vinfo,
-                             long long *__restrict__ big_items)
+                             long long n, int small_cap, int big_chunk, long long item_len,
+                             VInfo *__restrict__ vinfo, Counters *ctr,
+                             int2 *__restrict__ bitem, long long *__restrict__ irow)
 {
     long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
@@ -547,9 +533,61 @@ __global__ void vinfo_kernel(const OffT *__restrict__ off, const int *__restrict
     r.fbeg = (long long)off[v];
     r.fdeg = fcnt[v];
     const int d = deg[v];
-    r.key = rank ? rank[v] : d;
+    r.key = rank[v];
     vinfo[v] = r;
-    big_items[v] = (r.fdeg > small_cap) ? div_up<long long>(d, big_chunk) : 0;
+    post_row_items<OffT>(v, r.fbeg, r.fbeg + d, d, r.fdeg, small_cap, big_chunk, item_len, ctr,
+                         bitem, irow);
+}
+
+// Vertex-id labels: the whole forward build in one pass, a group of GS lanes
+// per row.  The group reads the row in GS-entry chunks, takes each
+// neighbour's degree from the offsets, keeps the entries ordered above the
+// row ((degree, id) order) and writes them, compacted by ballot, to the start
+// of the row's own CSR segment -- so every list keeps the row's ascending id
+// order and needs no sort.  The first lane then writes deg, fcnt, the
+// per-vertex record and the row's work items.
+template <typename OffT, int GS>
+__global__ void __launch_bounds__(256)
+row_place_kernel(const OffT *__restrict__ off, const int *__restrict__ ind, long long n,
+                 int *__restrict__ deg, int *__restrict__ fcnt, int *__restrict__ find,
+                 VInfo *__restrict__ vinfo, int small_cap, int big_chunk, long long item_len,
+                 Counters *ctr, int2 *__restrict__ bitem, long long *__restrict__ irow,
+                 unsigned int *status)
+{
+    auto grp = cg::tiled_partition<GS>(cg::this_thread_block());
+    const long long v = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / GS;
+    if (v >= n) return;                      // uniform across the group
+    const int lane = grp.thread_rank();
+    const long long b = (long long)off[v], e = (long long)off[v + 1];
+    const int dv = (int)(e - b);
+    int wrote = 0;
+    for (int k0 = 0; k0 < dv; k0 += GS) {
+        const int k = k0 + lane;
+        bool fwd = false;
+        int x = 0;
+        if (k < dv) {
+            x = ind[b + k];
+            if ((unsigned long long)(long long)x < (unsigned long long)n) {
+                const int dx = (int)((long long)off[x + 1] - (long long)off[x]);
+                fwd = dx > dv || (dx == dv && x > v);
+            } else {
+                atomicOr(status, kErrIndexRange);
+            }
+        }
+        const unsigned int m = grp.ballot(fwd);
+        if (fwd) find[b + wrote + __popc(m & ((1u << lane) - 1u))] = x;
+        wrote += __popc(m);
+    }
+    if (lane == 0) {
+        deg[v] = dv;
+        fcnt[v] = wrote;
+        VInfo r;
+        r.fbeg = b;
+        r.fdeg = wrote;
+        r.key = dv;
+        vinfo[v] = r;
+        post_row_items<OffT>(v, b, e, dv, wrote, small_cap, big_chunk, item_len, ctr, bitem, irow);
+    }
 }
 
 // ============================================================ intersection
@@ -676,47 +714,26 @@ probe_stride(const Grp &grp, long long s, long long end, int a, int ka, int fa, 
         const int px = grp.shfl(x, src);
         unsigned int hx = 0;
         if (TRIM) {
-            // The members ranked above the apex are a suffix of the sorted
-            // list.  One sampled load finds how many whole G-element chunks,
-            // counted from the end, lie above ka (lane k reads the first
-            // element of chunk k); those are swept without a per-element
-            // test, kTrimLoads chunks in flight, and only the chunk that
-            // holds the cut is masked.
-            int top = len;
-            while (top > 0) {
-                const int js = top - G * (lane + 1);
-                const int smp = js >= 0 ? list[js] : ka;
-                const int nfull = __popc(grp.ballot(smp > ka));
-                const int stop = top - G * nfull;
-                for (int base = top; base > stop; base -= kTrimLoads * G) {
-                    int w[kTrimLoads];
+            // windows of kTrimLoads * G elements from the end, all loads of a
+            // window in flight together
+            for (int top = len; top > 0; top -= kTrimLoads * G) {
+                int w[kTrimLoads];
 #pragma unroll
-                    for (int u = 0; u < kTrimLoads; ++u) {
-                        const int j = base - (u + 1) * G + lane;
-                        w[u] = j >= stop ? list[j] : -1;      // ranks are >= 0
-                    }
+                for (int u = 0; u < kTrimLoads; ++u) {
+                    const int j = top - (u + 1) * G + lane;
+                    w[u] = j >= 0 ? list[j] : ka;
+                }
 #pragma unroll
-                    for (int u = 0; u < kTrimLoads; ++u) {
-                        if (w[u] >= 0) {
-                            const int sl = lookup(w[u]);
-                            if (sl >= 0) {
-                                ++hx;
-                                if (PER_VERTEX) on_hit(sl, w[u]);
-                            }
-                        }
+                for (int u = 0; u < kTrimLoads; ++u) {
+                    const int sl = w[u] > ka ? lookup(w[u]) : -1;
+                    if (sl >= 0) {
+                        ++hx;
+                        if (PER_VERTEX) on_hit(sl, w[u]);
                     }
                 }
-                top = stop;
-                if (nfull < G) break;
-            }
-            if (top > 0) {                       // the chunk holding the cut
-                const int j = top - G + lane;
-                const int w0 = j >= 0 ? list[j] : ka;
-                const int sl = w0 > ka ? lookup(w0) : -1;
-                if (sl >= 0) {
-                    ++hx;
-                    if (PER_VERTEX) on_hit(sl, w0);
-                }
+                // sorted: once a loaded element is at or below ka, so is
+                // every element before it (lanes past the list start load ka)
+                if (grp.any(w[kTrimLoads - 1] <= ka)) break;
             }
         } else {
             int j = lane;
@@ -813,24 +830,6 @@ __device__ __forceinline__ void flush_hits(const ApexTable &tab, int tsize, int 
     }
 }
 
-// Work-item tables, so that no warp or block starts an item with a dependent
-// binary search: the first row of every warp work item (item k covers
-// entries [k*item_len, (k+1)*item_len)), and the (row, chunk) of every
-// block-kernel item (vertex v owns items big[v] .. big[v+1]-1, big being the
-// exclusive scan of its chunk counts).
-template <typename OffT>
-__global__ void item_rows_kernel(const OffT *__restrict__ off, long long n, long long item_len,
-                                 long long n_items, long long *__restrict__ irow,
-                                 const long long *__restrict__ big, int2 *__restrict__ bitem)
-{
-    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n_items) irow[k] = row_of_entry(off, n, k * item_len);
-    if (k < n) {
-        const long long b0 = big[k], b1 = big[k + 1];
-        for (long long c = b0; c < b1; ++c) bitem[c] = make_int2((int)k, (int)(c - b0));
-    }
-}
-
 // Shuffle co-rank: the lane i whose [incl_i - w_i, incl_i) holds f (incl is
 // this lane's inclusive prefix of a per-lane count; lanes with count 0 are
 // never returned for f < total).
@@ -888,12 +887,17 @@ __device__ __forceinline__ void region_insert(int *keys, int toff, int lg, int k
 //      the warp's shared table, placed by a prefix scan (rows that do not fit
 //      wait for the next batch);
 //   2. the rows' forward lists are inserted as one flattened stream;
-//   3. the rows' entries are scanned 32 at a time for partners, and each
-//      chunk's partner lists are probed as one flattened stream into the
-//      owning row's region (shuffle co-rank over the chunk's work prefix);
+//   3. the rows' entries are scanned 32 at a time for partners, which are
+//      appended to a per-warp queue in shared memory (list start, length,
+//      owning region); every 32 queued partners -- and the rest at the end
+//      of the batch -- are probed as one flattened stream into their apexes'
+//      regions (shuffle co-rank over the work prefix), so probe passes run
+//      full rather than once per entry chunk;
 //   4. a partner lane popcounts the hit ballot over its probe range and
-//      credits both itself and its apex; the per-slot 16-bit hit counters
-//      credit the third vertices in one flush per region.
+//      credits itself; apex credits collect in a shared per-row sum, and the
+//      per-slot 16-bit hit counters credit the third vertices, both flushed
+//      once per batch.
+// List positions are 32-bit when the offsets are (every position < 2^31).
 template <bool PER_VERTEX, typename OffT>
 __global__ void __launch_bounds__(kRowThreads, kRowMinBlocks)
 count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
@@ -905,12 +909,68 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                   const int *__restrict__ order)
 {
     constexpr int kWarps = kRowThreads / 32;
+    constexpr int kQueue = 64;                 // partner records per warp (32 + one chunk)
     __shared__ int s_keys[kWarps][kRowSlots];
     __shared__ unsigned int s_hits[kWarps][PER_VERTEX ? kRowSlots / 2 : 1];
+    using Pos = typename std::conditional<sizeof(OffT) == 4, int, long long>::type;
+    __shared__ Pos s_qfb[kWarps][kQueue];
+    __shared__ int s_qx[kWarps][kQueue], s_qfx[kWarps][kQueue], s_qrd[kWarps][kQueue];
+    __shared__ unsigned int s_apex[kWarps][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int *keys = s_keys[wid];
     unsigned int *hitw = s_hits[wid];
+    Pos *qfb = s_qfb[wid];
+    int *qx = s_qx[wid], *qfx = s_qfx[wid], *qrd = s_qrd[wid];
+    unsigned int *apex_sum = s_apex[wid];
+    apex_sum[lane] = 0;
+    __syncwarp();
     unsigned long long tri_local = 0;
+
+    // Probe the partner lists of queue records [0, k) (k <= 32) into their
+    // apexes' regions as one flattened stream; credits: the partner per lane,
+    // the apex through its batch row's shared sum.
+    auto probe_queue = [&](int k) {
+        int x = 0, fx = 0, rdp = 0;
+        Pos fb = 0;
+        if (lane < k) {
+            x = qx[lane];
+            fx = qfx[lane];
+            fb = qfb[lane];
+            rdp = qrd[lane];
+        }
+        __syncwarp();
+        const int pw = fx;
+        const int pincl = warp_incl_scan(pw);
+        const int ptot = __shfl_sync(0xffffffffu, pincl, 31);
+        const int pexcl = pincl - pw;
+        const Pos pbase = fb - pexcl;
+        unsigned int mine = 0;
+        for (int g0 = 0; g0 < ptot; g0 += 32) {
+            const int g = g0 + lane;
+            const int pp = warp_corank(pincl, g);
+            const Pos fb_p = __shfl_sync(0xffffffffu, pbase, pp);
+            const int rd_p = __shfl_sync(0xffffffffu, rdp, pp);
+            bool hit = false;
+            if (g < ptot) {
+                const int slot = region_find(keys, rd_p & 0xffff, (rd_p >> 16) & 0xff,
+                                             find[fb_p + g]);
+                if (slot >= 0) {
+                    hit = true;
+                    if (PER_VERTEX) atomicAdd(&hitw[slot >> 1], 1u << ((slot & 1) << 4));
+                }
+            }
+            const unsigned int hm = __ballot_sync(0xffffffffu, hit);
+            if (pw > 0) {
+                const int lo = max(pexcl - g0, 0), hi = min(pincl - g0, 32);
+                if (lo < hi) mine += __popc(hm & lane_range(lo, hi));
+            }
+        }
+        if (PER_VERTEX && mine) {
+            atomicAdd(&tacc[x], (unsigned long long)mine);
+            atomicAdd(&apex_sum[(rdp >> 24) & 31], mine);
+        }
+        tri_local += mine;
+    };
 
     while (true) {
         long long item = 0;
@@ -937,7 +997,8 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
             const int ts = act ? (1 << lg) : 0;
             const int tincl = warp_incl_scan(ts);
             const int toff = tincl - ts;
-            const int rdesc = toff | (lg << 16);      // region: offset | log2(size) << 16
+            // region: offset | log2(size) << 16 | batch row << 24
+            const int rdesc = toff | (lg << 16) | (lane << 24);
             const bool take = in_item && tincl <= kRowSlots;
             const unsigned int tmask = __ballot_sync(0xffffffffu, take);
             const int nrows = __popc(tmask);          // a prefix of the lanes
@@ -957,9 +1018,10 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                 for (int f0 = 0; f0 < ftot; f0 += 32) {
                     const int f = f0 + lane;
                     const int i = warp_corank(fincl, f);
-                    const long long fb_i = __shfl_sync(0xffffffffu, vi.fbeg - fexcl, i);
+                    const Pos fb_i = __shfl_sync(0xffffffffu, (Pos)vi.fbeg - fexcl, i);
                     const int rd_i = __shfl_sync(0xffffffffu, rdesc, i);
-                    if (f < ftot) region_insert(keys, rd_i & 0xffff, rd_i >> 16, find[fb_i + f]);
+                    if (f < ftot)
+                        region_insert(keys, rd_i & 0xffff, (rd_i >> 16) & 0xff, find[fb_i + f]);
                 }
                 __syncwarp();
                 // ---- 3. scan the active rows' entries for partners, probe
@@ -967,68 +1029,63 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                 const int lincl = warp_incl_scan(lw);
                 const int ltot = __shfl_sync(0xffffffffu, lincl, 31);
                 const int lexcl = lincl - lw;
+                int qn = 0;
                 for (int c0 = 0; c0 < ltot; c0 += 32) {
                     const int f = c0 + lane;
                     const int i = warp_corank(lincl, f);
-                    const long long s0_i = __shfl_sync(0xffffffffu, s0 - lexcl, i);
+                    const Pos s0_i = __shfl_sync(0xffffffffu, (Pos)s0 - lexcl, i);
                     const int fa_i = __shfl_sync(0xffffffffu, vi.fdeg, i);
                     const int ka_i = __shfl_sync(0xffffffffu, vi.key, i);
                     const int rd_i = __shfl_sync(0xffffffffu, rdesc, i);
                     const int a = (int)(ra + i);
                     bool partner = false;
                     int x = 0, fx = 0;
-                    long long fbx = 0;
+                    Pos fbx = 0;
                     if (f < ltot) {
                         x = ind[s0_i + f];
                         if ((unsigned long long)(long long)x < (unsigned long long)n) {
                             const VInfo ix = vinfo[x];
                             fx = ix.fdeg;
-                            fbx = ix.fbeg;
+                            fbx = (Pos)ix.fbeg;
                             const bool fwd = rank_above(ix.key, x, ka_i, a);
                             partner = fx > 0 && (fwd ? fx <= fa_i : fx < fa_i);
                         } else {
                             atomicOr(status, kErrIndexRange);
                         }
                     }
-                    const int pw = partner ? fx : 0;
-                    const int pincl = warp_incl_scan(pw);
-                    const int ptot = __shfl_sync(0xffffffffu, pincl, 31);
-                    const int pexcl = pincl - pw;
-                    unsigned int mine = 0;
-                    const long long pbase = fbx - pexcl;      // list base minus its probe offset
-                    for (int g0 = 0; g0 < ptot; g0 += 32) {
-                        const int g = g0 + lane;
-                        const int p = warp_corank(pincl, g);
-                        const long long fb_p = __shfl_sync(0xffffffffu, pbase, p);
-                        const int rd_p = __shfl_sync(0xffffffffu, rd_i, p);
-                        bool hit = false;
-                        if (g < ptot) {
-                            const int slot = region_find(keys, rd_p & 0xffff, rd_p >> 16, find[fb_p + g]);
-                            if (slot >= 0) {
-                                hit = true;
-                                if (PER_VERTEX) atomicAdd(&hitw[slot >> 1], 1u << ((slot & 1) << 4));
-                            }
-                        }
-                        const unsigned int hm = __ballot_sync(0xffffffffu, hit);
-                        if (pw > 0) {
-                            const int lo = max(pexcl - g0, 0), hi = min(pincl - g0, 32);
-                            if (lo < hi) mine += __popc(hm & lane_range(lo, hi));
-                        }
+                    // queue this chunk's partners; probe 32 at a time
+                    const unsigned int pm = __ballot_sync(0xffffffffu, partner);
+                    if (partner) {
+                        const int pos = qn + __popc(pm & ((1u << lane) - 1u));
+                        qx[pos] = x;
+                        qfx[pos] = fx;
+                        qfb[pos] = fbx;
+                        qrd[pos] = rd_i;
                     }
-                    // partner credits per lane; apex credits summed over the
-                    // lanes of each row first (one atomic per row and chunk)
-                    if (PER_VERTEX) {
-                        if (mine) atomicAdd(&tacc[x], (unsigned long long)mine);
-                        const unsigned int same = __match_any_sync(0xffffffffu, i);
-                        const unsigned int rsum = __reduce_add_sync(same, mine);
-                        if (rsum && lane == __ffs(same) - 1)
-                            atomicAdd(&tacc[a], (unsigned long long)rsum);
+                    qn += __popc(pm);
+                    __syncwarp();
+                    if (qn >= 32) {
+                        probe_queue(32);
+                        const int rest = qn - 32;
+                        if (lane < rest) {
+                            qx[lane] = qx[32 + lane];
+                            qfx[lane] = qfx[32 + lane];
+                            qfb[lane] = qfb[32 + lane];
+                            qrd[lane] = qrd[32 + lane];
+                        }
+                        __syncwarp();
+                        qn = rest;
                     }
-                    tri_local += mine;
                 }
+                if (qn > 0) probe_queue(qn);
                 __syncwarp();
-                // ---- 4. third-vertex credits
+                // ---- 4. third-vertex and apex credits
                 if (PER_VERTEX) {
+                    const unsigned int as = apex_sum[lane];
+                    if (as) {
+                        atomicAdd(&tacc[ra + lane], (unsigned long long)as);
+                        apex_sum[lane] = 0;
+                    }
                     for (int k = lane; k < (total_slots >> 1); k += 32) {
                         const unsigned int pair = hitw[k];
                         if (pair) {
@@ -1073,14 +1130,13 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
 // Within an item the warps take 32-entry strides from a shared counter, so
 // uneven partner work does not idle the block at its barriers.
 template <bool PER_VERTEX, typename OffT, bool RANK>
-__global__ void __launch_bounds__(kBigThreads)
+__global__ void __launch_bounds__(kBigThreads, kBigMinBlocks)
 count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                  long long n, const VInfo *__restrict__ vinfo,
                  const int *__restrict__ find,
                  unsigned long long *__restrict__ tacc, Counters *ctr,
-                 unsigned int *status, const long long *__restrict__ big_pre,
-                 const int2 *__restrict__ bitem, int big_chunk, int big_hash_max,
-                 int small_cap, const int *__restrict__ order)
+                 unsigned int *status, const int2 *__restrict__ bitem, int big_chunk,
+                 int big_hash_max, int small_cap, const int *__restrict__ order)
 {
     extern __shared__ int smem[];
     int *keys = smem;
@@ -1092,7 +1148,7 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
     auto block = cg::this_thread_block();
     auto warp = cg::tiled_partition<32>(block);
     const int lane = warp.thread_rank();
-    const long long n_items = big_pre[n];
+    const long long n_items = (long long)ctr->big_total;
     unsigned long long tri_local = 0;
 
     while (true) {
@@ -1338,14 +1394,10 @@ Plan make_plan(long long n, long long nnz, int off_bits, bool per_vertex)
     p.o_deg = take(sizeof(int) * (size_t)n);
     p.o_rank = take(sizeof(int) * (size_t)n);
     p.o_order = take(sizeof(int) * (size_t)n);
-    p.o_tile = take(sizeof(long long) * (size_t)(p.n_tiles + 1));
-    long long scan_n = p.n_tiles > n ? p.n_tiles : n;
-    p.o_scan_tmp = take(scan_tmp_bytes(scan_n));
     p.o_fcnt = take(sizeof(int) * (size_t)n);
     p.o_vinfo = take(sizeof(VInfo) * (size_t)n);
     p.o_find = take(sizeof(int) * (size_t)(p.fwd_cap + 4));
     p.o_tacc = take(per_vertex ? sizeof(unsigned long long) * (size_t)n : 0);
-    p.o_big = take(sizeof(long long) * (size_t)(n + 1));
     p.o_trow = take(sizeof(long long) * (size_t)(p.n_tiles + 1));
     p.o_irow = take(sizeof(long long) * (size_t)(div_up<long long>(nnz, kMinItemLen) + 1));
     // block-kernel items: at most one per row plus one per kMinBigChunk entries
@@ -1400,10 +1452,11 @@ gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
 
 int launches_per_count(const RowConfig &cfg, bool per_vertex)
 {
-    // degree, tile bounds, tile place, list sort (split rows with vertex
-    // ids), vinfo, scan x3, item rows, warp kernel, block kernel, global;
-    // finalize (per vertex); rank scan and rank (rank labels)
-    return 12 + (per_vertex ? 1 : 0) + (cfg.rank_labels ? 2 : 0);
+    // vertex-id labels: row placement; rank labels: degree histogram, rank
+    // scan, rank, tile bounds, tile placement, list sort, vinfo.  Then the
+    // warp kernel, the block kernel, the global count and, per vertex,
+    // finalize.
+    return (cfg.rank_labels ? 7 : 1) + 3 + (per_vertex ? 1 : 0);
 }
 
 template <typename OffT>
@@ -1419,12 +1472,10 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
     unsigned int *status = reinterpret_cast<unsigned int *>(base + p.o_status);
     Counters *ctr = reinterpret_cast<Counters *>(base + p.o_counters);
     int *deg = reinterpret_cast<int *>(base + p.o_deg);
-    void *scan_tmp = base + p.o_scan_tmp;
     int *fcnt = reinterpret_cast<int *>(base + p.o_fcnt);
     VInfo *vinfo = reinterpret_cast<VInfo *>(base + p.o_vinfo);
     int *find = reinterpret_cast<int *>(base + p.o_find);
     unsigned long long *tacc = reinterpret_cast<unsigned long long *>(base + p.o_tacc);
-    long long *big = reinterpret_cast<long long *>(base + p.o_big);
     long long *trow = reinterpret_cast<long long *>(base + p.o_trow);
     long long *irow = reinterpret_cast<long long *>(base + p.o_irow);
     int2 *bitem = reinterpret_cast<int2 *>(base + p.o_bitem);
@@ -1448,25 +1499,16 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
         const unsigned vb = (unsigned)div_up<long long>(n, 256);
         if (timing) cudaEventRecord(timing->ev[0], stream);
         nvtxRangePushA("gtc: forward lists");
+        const int small_cap = 4 * cfg.group;   // <= kRowSlots / 8
         if (rank_labels) {
             const unsigned rb = (unsigned)div_up<long long>(n, kRankChunk);
             degree_hist_kernel<<<rb, kRankThreads, 0, stream>>>(off, off_bits, n, deg, hist);
             rank_scan_kernel<<<1, kRankScanThreads, 0, stream>>>(hist);
             rank_kernel<<<rb, kRankThreads, 0, stream>>>(deg, n, hist, rank, order);
-        } else {
-            degree_kernel<<<vb, 256, 0, stream>>>(off, off_bits, n, deg);
-        }
-        tile_bounds_kernel<OffT><<<(unsigned)div_up<long long>(p.n_tiles + 1, 256), 256, 0,
-                                   stream>>>(off, n, nnz, p.n_tiles, trow, fcnt);
-        const unsigned nt = (unsigned)p.n_tiles;
-        if (rank_labels) {
-            tile_place_kernel<OffT, true><<<nt, kPrepThreads, 0, stream>>>(
+            tile_bounds_kernel<OffT><<<(unsigned)div_up<long long>(p.n_tiles + 1, 256), 256, 0,
+                                       stream>>>(off, n, nnz, p.n_tiles, trow, fcnt);
+            tile_place_kernel<OffT, true><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
                 off, ind, rank, n, nnz, trow, fcnt, find, status);
-        } else {
-            tile_place_kernel<OffT, false><<<nt, kPrepThreads, 0, stream>>>(
-                off, ind, deg, n, nnz, trow, fcnt, find, status);
-        }
-        if (rank_labels) {
             // rank order for the lists read in order (rows hold their members
             // in id order)
             long long sb = occupancy_blocks(sort_lists_kernel<OffT>, kSortThreads, 0, dev,
@@ -1475,27 +1517,28 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
             if (sneed < sb) sb = sneed;
             sort_lists_kernel<OffT><<<(unsigned)sb, kSortThreads, 0, stream>>>(
                 off, fcnt, n, find, ctr, min(4 * cfg.group, 31));
-        } else if (p.n_tiles > 1) {
-            // id order (the block kernel binary-searches lists above
-            // big_hash_max): only rows split between tiles can be out of order
-            sort_split_rows_kernel<OffT><<<(unsigned)div_up<long long>(p.n_tiles - 1,
-                                                                       kSortThreads / 32),
-                                           kSortThreads, 0, stream>>>(off, fcnt, trow, p.n_tiles,
-                                                                      n, find);
+            vinfo_kernel<OffT><<<vb, 256, 0, stream>>>(off, fcnt, deg, rank, n, small_cap,
+                                                       cfg.big_chunk, cfg.item_len, vinfo, ctr,
+                                                       bitem, irow);
+        } else {
+            // one row per group of gs lanes, gs ~ the mean degree
+            const double mean = (double)nnz / (double)n;
+            const int gs = mean <= 8.0 ? 8 : (mean <= 16.0 ? 16 : 32);
+            const unsigned pb = (unsigned)div_up<long long>(n * gs, 256);
+            auto place = [&](auto kern) {
+                kern<<<pb, 256, 0, stream>>>(off, ind, n, deg, fcnt, find, vinfo, small_cap,
+                                             cfg.big_chunk, cfg.item_len, ctr, bitem, irow,
+                                             status);
+            };
+            if (gs == 8) place(row_place_kernel<OffT, 8>);
+            else if (gs == 16) place(row_place_kernel<OffT, 16>);
+            else place(row_place_kernel<OffT, 32>);
         }
-        const int small_cap = 4 * cfg.group;   // <= kRowSlots / 8
-        vinfo_kernel<OffT><<<vb, 256, 0, stream>>>(off, fcnt, deg, rank_labels ? rank : nullptr, n,
-                                                   small_cap, cfg.big_chunk, vinfo, big);
-        err = exclusive_scan_i64(big, big, n, scan_tmp, stream);
         nvtxRangePop();
-        if (err != cudaSuccess) return GTC_ERR_CUDA;
         if (timing) cudaEventRecord(timing->ev[1], stream);
         const int *lorder = rank_labels ? order : nullptr;
         if (nnz > 0) {
             const long long n_items = div_up<long long>(nnz, cfg.item_len);
-            const long long it_threads = n_items > n ? n_items : n;
-            item_rows_kernel<OffT><<<(unsigned)div_up<long long>(it_threads, 256), 256, 0,
-                                     stream>>>(off, n, cfg.item_len, n_items, irow, big, bitem);
             auto launch_rows = [&](auto kern) {
                 int blocks = occupancy_blocks(kern, kRowThreads, 0, dev,
                                               &g_rows_blocks[dev & 63][per_vertex ? 1 : 0]);
@@ -1517,7 +1560,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                 cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem);
                 int blocks = occupancy_blocks(kern, kBigThreads, big_smem, dev, cache);
                 kern<<<blocks, kBigThreads, big_smem, stream>>>(off, ind, n, vinfo, find, tacc, ctr,
-                                                                status, big, bitem, cfg.big_chunk,
+                                                                status, bitem, cfg.big_chunk,
                                                                 cfg.big_hash_max, small_cap, lorder);
             };
             int *bc = g_big_blocks[dev & 63];

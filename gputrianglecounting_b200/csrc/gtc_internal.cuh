@@ -40,13 +40,12 @@ constexpr int kRowSlots = 512;              // shared table slots per warp
 constexpr int kRowMinBlocks = 6;            // 48 warps per SM (register budget 42)
 constexpr int kMinItemLen = 32;             // smallest warp work item (entries)
 constexpr int kMaxItemLen = 65535;          // largest: a 16-bit hit counter must not carry
-constexpr int kBigThreads = 256;            // block-per-row count kernel (8 blocks/SM)
+constexpr int kBigThreads = 256;            // block-per-row count kernel
+constexpr int kBigMinBlocks = 8;            // 8 blocks (64 warps) per SM: 32 registers
 constexpr int kMinBigChunk = 32;            // smallest block-kernel item (entries)
 constexpr int kBigTableLog2 = 12;
 constexpr int kBigTableSlots = 1 << kBigTableLog2;   // shared hash slots (block kernel)
 constexpr int kBigHashMaxFdeg = 2048;       // longest list hashed (load <= 1/2)
-
-constexpr int kScanThreads = 1024;
 
 // Degree-rank labels (skewed graphs): vertices are ordered by degree (a
 // counting sort over kRankBuckets degree buckets; degrees above the last
@@ -125,9 +124,8 @@ struct Plan {
     long long n_tiles = 0;       // merge-path tiles over rows + entries
     long long fwd_cap = 0;       // capacity of the forward adjacency
     // workspace byte offsets
-    size_t o_status = 0, o_counters = 0, o_deg = 0, o_tile = 0, o_scan_tmp = 0,
-           o_fcnt = 0, o_vinfo = 0, o_find = 0, o_tacc = 0, o_big = 0,
-           o_bigpre = 0, o_trow = 0, o_irow = 0, o_hist = 0, o_rank = 0, o_order = 0,
+    size_t o_status = 0, o_counters = 0, o_deg = 0, o_fcnt = 0, o_vinfo = 0, o_find = 0,
+           o_tacc = 0, o_trow = 0, o_irow = 0, o_hist = 0, o_rank = 0, o_order = 0,
            o_bitem = 0;
     size_t bytes = 0;
 };
@@ -139,12 +137,9 @@ struct Counters {
     unsigned long long big_items;     // dynamic item queue, block kernel
     unsigned long long big_rows;      // number of rows for the block kernel
     unsigned long long sort_groups;   // dynamic queue of 32-row groups, list sort
-    unsigned long long pad[3];
+    unsigned long long big_total;     // block-kernel items posted by the forward build
+    unsigned long long pad[2];
 };
 
-size_t scan_tmp_bytes(long long count);
-cudaError_t exclusive_scan_i64(const long long *in, long long *out,
-                               long long count, void *tmp,
-                               cudaStream_t stream);
 
 }  // namespace gtc
