@@ -396,12 +396,20 @@ def run_b200(args, name: str, rank: int, world: int, with_baseline: bool = True)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
 
-    # warm-up (also validates the input once)
+    # warm-up (also validates the input once); the launch shape comes from the
+    # autotuner (staged search, cached per degree profile), chosen before any
+    # timed step
     reason, why = api.validate_csr(g.off, g.ind)
     if reason != 0:
         raise RuntimeError(f"generated graph invalid: {why}")
+    from gputrianglecounting_b200 import autotune
+    t_tune = time.perf_counter()
+    tuning = autotune.autotune(g.off, g.ind, counter=counter, search="staged",
+                               cache_path=args.tune_cache)
+    tune_s = time.perf_counter() - t_tune
+    tune_entry = autotune.tuned_entry(g.off, g.nnz) or {}
     for _ in range(args.warmup):
-        out = counter.count(g.off, g.ind, out=out)
+        out = counter.count(g.off, g.ind, out=out, tuning=tuning)
     torch.cuda.synchronize()
 
     # device-timed steps, one event pair per step, L2 flushed between steps
@@ -414,7 +422,7 @@ def run_b200(args, name: str, rank: int, world: int, with_baseline: bool = True)
         for k in range(args.steps):
             flush.fill_(k & 0xff)
             evs[k][0].record(stream)
-            out = counter.count(g.off, g.ind, out=out)
+            out = counter.count(g.off, g.ind, out=out, tuning=tuning)
             evs[k][1].record(stream)
         torch.cuda.synchronize()
     if world > 1:
@@ -424,7 +432,7 @@ def run_b200(args, name: str, rank: int, world: int, with_baseline: bool = True)
     T = out.triangles
 
     # phase breakdown of one count (events between the pipeline phases)
-    phases = phase_breakdown(counter, g, flush)
+    phases = phase_breakdown(counter, g, flush, tuning)
 
     # end to end through the public API with host buffers (pinned), copies
     # inside the timed region
@@ -443,7 +451,7 @@ def run_b200(args, name: str, rank: int, world: int, with_baseline: bool = True)
             e2e_evs[k - args.warmup][0].record(stream)
         d_off.copy_(h_off, non_blocking=True)
         d_ind.copy_(h_ind, non_blocking=True)
-        res = counter.count(d_off, d_ind, outputs=("r", "lcc"))
+        res = counter.count(d_off, d_ind, outputs=("r", "lcc"), tuning=tuning)
         h_r.copy_(res.r, non_blocking=True)
         h_lcc.copy_(res.lcc, non_blocking=True)
         h_glob.copy_(res.global_counts, non_blocking=True)
@@ -472,6 +480,9 @@ def run_b200(args, name: str, rank: int, world: int, with_baseline: bool = True)
         "dtype": DTYPE, "data": "synthetic",
         "config": graph_config(name, cfg, host, world),
         "result": {"triangles": T},
+        "tuning": {"launch_shape": tuning, "search_s": tune_s,
+                   "untuned_ms": tune_entry.get("default_ms"),
+                   "tuned_ms": tune_entry.get("ms")},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": (traffic or {}).get("bytes"),
@@ -491,7 +502,7 @@ def run_b200(args, name: str, rank: int, world: int, with_baseline: bool = True)
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms / args.steps},
         "clocks": clk.result,
-        "gpu_launches": launches_per_count(host.n, host.nnz) * args.steps,
+        "gpu_launches": launches_per_count(host.n, host.nnz, tuning) * args.steps,
     }
     if with_baseline and not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -515,10 +526,10 @@ def int32_offsets(host_graph):
                     host_graph.name)
 
 
-def phase_breakdown(counter, g, flush) -> dict:
-    """Per-phase device time of one count, from events the library records
-    between its phases (forward build / group kernel / block kernel /
-    epilogue), averaged over 3 runs."""
+def phase_breakdown(counter, g, flush, tuning: dict | None = None) -> dict:
+    """Per-phase device time of one count with this tuning, from events the
+    library records between its phases (forward build / group kernel / block
+    kernel / epilogue), averaged over 3 runs."""
     import ctypes
 
     import torch
@@ -527,12 +538,13 @@ def phase_breakdown(counter, g, flush) -> dict:
     n, nnz = g.off.numel() - 1, g.ind.numel()
     off_bits = 32 if g.off.dtype == torch.int32 else 64
     ws = counter._workspace(counter.workspace_bytes(n, nnz, off_bits))
+    tun = _lib.Tuning(**{k: int(v) for k, v in tuning.items()}) if tuning else None
     res = []
     for k in range(3):
         flush.fill_(k)
         times = (ctypes.c_float * 4)()
         st = fn(g.off.data_ptr(), off_bits, g.ind.data_ptr(), n, nnz, ws.data_ptr(), ws.numel(),
-                ctypes.cast(times, ctypes.c_void_p))
+                ctypes.cast(times, ctypes.c_void_p), ctypes.byref(tun) if tun else None)
         _lib.check(st, "gtc_count_phase_times")
         res.append(list(times))
     torch.cuda.synchronize()
@@ -545,8 +557,13 @@ def phase_breakdown(counter, g, flush) -> dict:
 
 def batch_launches(total_n: int, total_nnz: int, tuning: dict | None = None) -> int:
     """Entry starts + globalize + the pipeline without its global-count
-    kernel + per-graph T."""
-    return 2 + (launches_per_count(total_n, total_nnz, tuning) - 1) + 1
+    kernel + per-graph T; with degree-rank labels the batch's graph-major
+    ranks take a histogram, a 3-launch scan and a rank kernel in place of the
+    single graph's 3 rank launches (+2)."""
+    from gputrianglecounting_b200 import api
+    extra = 2 if api.launch_plan(total_n, total_nnz, tuning=tuning)["labels"] == "degree-rank" \
+        else 0
+    return 2 + (launches_per_count(total_n, total_nnz, tuning) - 1) + 1 + extra
 
 
 def run_batched(args, cfg, rank: int, world: int):
@@ -574,7 +591,7 @@ def run_batched(args, cfg, rank: int, world: int):
     # before any timed step
     from gputrianglecounting_b200 import autotune
     t0 = time.perf_counter()
-    tuning = autotune.autotune_batch(bc, batch, out=out)
+    tuning = autotune.autotune_batch(bc, batch, out=out, cache_path=args.tune_cache)
     tune_s = time.perf_counter() - t0
     tune_entry = autotune.batch_entry(batch)
     stream = torch.cuda.Stream(dev)
@@ -689,7 +706,8 @@ def run_serving(args, cfg, rank: int, world: int):
     torch.cuda.synchronize()
     # launch shape tuned once on the pool's union (the typical admitted batch)
     from gputrianglecounting_b200 import api, autotune
-    tuning = autotune.autotune_batch(api.BatchCounter(dev), G.concat_graphs(pool, dev))
+    tuning = autotune.autotune_batch(api.BatchCounter(dev), G.concat_graphs(pool, dev),
+                                     cache_path=args.tune_cache)
     server = serve.CountServer(graphs, dev, slots=3, budget_bytes=4 << 30, max_graphs=512,
                                tuning=tuning)
     # warm-up: every graph once, to size the slots' workspaces
@@ -735,6 +753,9 @@ def main() -> None:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="rmat20")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune-cache", default=None,
+                    help="JSON file caching the autotuner's launch shapes per degree profile "
+                         "(read if present, written after a search)")
     ap.add_argument("--no-extras", action="store_true",
                     help="default workload only: skip the batched and serving sub-runs")
     args = ap.parse_args()
@@ -771,7 +792,8 @@ def main() -> None:
                     if line is not None:
                         line[other] = {"edges_per_s": o["value"], "ms": o["ms_per_step"],
                                        "steps": o["steps"], "config": o["config"],
-                                       "result": o["result"], "roofline": o["roofline"],
+                                       "result": o["result"], "tuning": o["tuning"],
+                                       "roofline": o["roofline"],
                                        "phases_ms": o["phases_ms"], "e2e": o["e2e"],
                                        "clocks": o["clocks"]}
                         if "cpu_baseline" in o:

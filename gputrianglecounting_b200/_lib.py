@@ -37,7 +37,7 @@ _SIGNATURES = {
                                 P]),
     "gtc_count_launches": (c_int, [c_int64, c_int64, c_int, P, P, P]),
     "gtc_count_status": (c_int, [P, c_size_t, P, P]),
-    "gtc_count_phase_times": (c_int, [P, c_int, P, c_int64, c_int64, P, c_size_t, P]),
+    "gtc_count_phase_times": (c_int, [P, c_int, P, c_int64, c_int64, P, c_size_t, P, P]),
     "gtc_count_noalloc": (c_int, [P, c_int, P, c_int64, c_int64, c_int, P, P, P, P, P]),
     "gtc_batch_workspace_size": (c_int, [c_int64, c_int64, c_int64, P]),
     "gtc_count_batch": (c_int, [c_int64, P, P, P, c_int64, c_int64, P, P, P, P, P, c_size_t, P,

@@ -408,17 +408,19 @@ gtc_status gtc_count(const void *d_off, int off_bits, const int32_t *d_ind, int6
 
 gtc_status gtc_count_phase_times(const void *d_off, int off_bits, const int32_t *d_ind,
                                  int64_t n, int64_t nnz, void *d_workspace, size_t ws_bytes,
-                                 float *h_ms)
+                                 float *h_ms, const gtc_tuning *tuning)
 {
     size_t need = 0;
     gtc_status st = gtc_workspace_size(n, nnz, off_bits, GTC_MODE_PLAIN, &need);
     if (st != GTC_OK) return st;
     if (!d_off || (nnz > 0 && !d_ind) || !d_workspace || !h_ms) return GTC_ERR_INVALID_ARGUMENT;
     if (ws_bytes < need) return GTC_ERR_WORKSPACE_TOO_SMALL;
+    RowConfig cfg = pick_row_config(n, nnz);
+    st = apply_tuning(cfg, tuning);
+    if (st != GTC_OK) return st;
     CountTimings tm;
     for (int i = 0; i < 5; ++i)
         if (cudaEventCreate(&tm.ev[i]) != cudaSuccess) return GTC_ERR_CUDA;
-    RowConfig cfg = pick_row_config(n, nnz);
     if (off_bits == 32)
         st = run_count<int>(static_cast<const int *>(d_off), d_ind, n, nnz, true, nullptr,
                             nullptr, nullptr, nullptr, d_workspace, ws_bytes, 0, cfg, &tm);

@@ -6,8 +6,12 @@
 // (0 .. n_g-1).  The batch entry point turns local ids into union ids in one
 // pass and runs the single-graph pipeline (persistent kernels pulling work
 // items from device queues) once over the union; triangles never cross graphs,
-// so every per-vertex value is exactly the one the graph gets alone.  A final
-// kernel sums t over each graph's vertex range into that graph's T.
+// so every per-vertex value is exactly the one the graph gets alone.  With
+// degree-rank labels the ranks are graph-major (each graph's vertices take the
+// consecutive ranks vstart[g] ..), so an apex's forward list spans only its own
+// graph's ranks and small graphs keep the block kernel's direct per-rank
+// counters.  A final kernel sums t over each graph's vertex range into that
+// graph's T.
 // The reference has no batched form; its per-graph operator is kernelCall
 // (src/clusteringCount.cu:415-467), which the one-launch-per-graph baseline
 // calls once per graph.
@@ -129,7 +133,8 @@ __global__ void pack_entries_kernel(const PackRef *__restrict__ refs,
 
 struct BatchPlan {
     Plan inner;               // the union graph's pipeline workspace
-    size_t o_estart = 0, o_indg = 0, o_inner = 0, bytes = 0;
+    size_t o_estart = 0, o_indg = 0, o_inner = 0, o_ghist = 0, o_scan = 0, o_rend = 0,
+           bytes = 0;
 };
 
 inline size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -144,6 +149,10 @@ BatchPlan make_batch_plan(long long G, long long total_n, long long total_nnz)
     b.o_inner = o;  o = align256(o + b.inner.bytes);
     b.o_estart = o; o = align256(o + sizeof(long long) * (size_t)(G + 1));
     b.o_indg = o;   o = align256(o + sizeof(int) * (size_t)(total_nnz + 1));
+    // graph-major degree ranks: per-graph bucket histogram and its scan
+    b.o_ghist = o;  o = align256(o + sizeof(long long) * (size_t)(G * kSegBuckets + 1));
+    b.o_scan = o;   o = align256(o + scan_tmp_bytes(G * kSegBuckets));
+    b.o_rend = o;   o = align256(o + sizeof(int) * (size_t)(total_n + 1));
     b.bytes = o;
     return b;
 }
@@ -197,10 +206,16 @@ gtc_status gtc_count_batch(int64_t num_graphs, const int64_t *d_vstart, const in
         globalize_kernel<<<(unsigned)div_up<long long>(total_nnz, kChunk), 256, 0, s>>>(
             estart, vstart, num_graphs, d_ind, ind_g, total_nnz);
     if (cudaGetLastError() != cudaSuccess) return GTC_ERR_CUDA;
+    SegRanks seg;
+    seg.vstart = vstart;
+    seg.num_graphs = num_graphs;
+    seg.ghist = reinterpret_cast<long long *>(base + b.o_ghist);
+    seg.scan_tmp = base + b.o_scan;
+    seg.rank_end = reinterpret_cast<int *>(base + b.o_rend);
     st = run_count<long long>(off, ind_g, total_n, total_nnz, true,
                               reinterpret_cast<long long *>(d_r),
                               reinterpret_cast<long long *>(d_t), d_lcc, nullptr, inner,
-                              b.inner.bytes, s, cfg, nullptr);
+                              b.inner.bytes, s, cfg, nullptr, &seg);
     if (st != GTC_OK) return st;
     if (d_graph_T) {
         const unsigned long long *tacc =

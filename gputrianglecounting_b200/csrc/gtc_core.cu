@@ -138,6 +138,75 @@ rank_kernel(const int *__restrict__ deg, long long n, unsigned long long *__rest
     }
 }
 
+// ---- graph-major degree ranks of a batch (SegRanks)
+
+// Graph holding vertex v: the largest g < G with vstart[g] <= v.
+__device__ __forceinline__ long long seg_of(const long long *__restrict__ vstart, long long G,
+                                            long long v)
+{
+    long long lo = 0, hi = G;
+    while (hi - lo > 1) {
+        const long long mid = (lo + hi) >> 1;
+        if (vstart[mid] <= v) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ long long seg_key(const long long *__restrict__ vstart, long long G,
+                                             long long v, int d)
+{
+    return seg_of(vstart, G, v) * kSegBuckets + (d < kSegBuckets ? d : kSegBuckets - 1);
+}
+
+// deg[v] and the per-graph degree-bucket histogram ghist[g * kSegBuckets + b]
+// (warp-aggregated global atomics).
+template <typename OffT>
+__global__ void seg_degree_hist_kernel(const OffT *__restrict__ off, long long n,
+                                       const long long *__restrict__ vstart, long long G,
+                                       int *__restrict__ deg, unsigned long long *ghist)
+{
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    long long key = -1;
+    if (v < n) {
+        const int d = (int)((long long)off[v + 1] - (long long)off[v]);
+        deg[v] = d;
+        key = seg_key(vstart, G, v, d);
+    }
+    const unsigned int peers = __match_any_sync(0xffffffffu, key);
+    if (v < n && lane == __ffs(peers) - 1)
+        atomicAdd(&ghist[key], (unsigned long long)__popc(peers));
+}
+
+// rank[v] = start of its (graph, bucket) + arrival in it; order[rank] = v;
+// rank_end[v] = the end of v's graph's ranks.  cursor = the exclusive scan of
+// ghist, whose graph-major order places graph g's buckets at vstart[g].
+__global__ void seg_rank_kernel(const int *__restrict__ deg, long long n,
+                                const long long *__restrict__ vstart, long long G,
+                                unsigned long long *cursor, int *__restrict__ rank,
+                                int *__restrict__ order, int *__restrict__ rank_end)
+{
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    long long key = -1;
+    if (v < n) {
+        const long long g = seg_of(vstart, G, v);
+        const int d = deg[v];
+        key = g * kSegBuckets + (d < kSegBuckets ? d : kSegBuckets - 1);
+        rank_end[v] = (int)vstart[g + 1];    // the graph's ranks end where its vertices do
+    }
+    const unsigned int peers = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(peers) - 1;
+    unsigned long long at = 0;
+    if (v < n && lane == leader) at = atomicAdd(&cursor[key], (unsigned long long)__popc(peers));
+    at = __shfl_sync(0xffffffffu, at, leader);
+    if (v < n) {
+        const int r = (int)(at + __popc(peers & ((1u << lane) - 1u)));
+        rank[v] = r;
+        order[r] = (int)v;
+    }
+}
+
 // Rows consumed at merge-path diagonal `diag` of the merge of the row-end
 // offsets off[1..n] with the entry indices 0..nnz-1 (Merrill & Garland,
 // "Merge-based parallel sparse matrix-vector multiplication", SC'16).
@@ -507,7 +576,7 @@ sort_lists_kernel(const OffT *__restrict__ off, const int *__restrict__ fcnt, lo
 template <typename OffT>
 __device__ __forceinline__ void post_row_items(long long v, long long b, long long e, int d,
                                                int fdeg, int small_cap, int big_chunk,
-                                               long long item_len, Counters *ctr,
+                                               int item_shift, Counters *ctr,
                                                int2 *__restrict__ bitem,
                                                long long *__restrict__ irow)
 {
@@ -516,14 +585,16 @@ __device__ __forceinline__ void post_row_items(long long v, long long b, long lo
         const unsigned long long at = atomicAdd(&ctr->big_total, (unsigned long long)k);
         for (int c = 0; c < k; ++c) bitem[at + c] = make_int2((int)v, c);
     }
-    for (long long k = div_up<long long>(b, item_len); k * item_len < e; ++k) irow[k] = v;
+    // items whose first entry lies in [b, e) (item_len = 2^item_shift)
+    const long long mask = (1ll << item_shift) - 1;
+    for (long long k = (b + mask) >> item_shift; (k << item_shift) < e; ++k) irow[k] = v;
 }
 
 // Rank labels: per-vertex record and work items (one thread per vertex).
 template <typename OffT>
 __global__ void vinfo_kernel(const OffT *__restrict__ off, const int *__restrict__ fcnt,
                              const int *__restrict__ deg, const int *__restrict__ rank,
-                             long long n, int small_cap, int big_chunk, long long item_len,
+                             long long n, int small_cap, int big_chunk, int item_shift,
                              VInfo *__restrict__ vinfo, Counters *ctr,
                              int2 *__restrict__ bitem, long long *__restrict__ irow)
 {
@@ -535,7 +606,7 @@ __global__ void vinfo_kernel(const OffT *__restrict__ off, const int *__restrict
     const int d = deg[v];
     r.key = rank[v];
     vinfo[v] = r;
-    post_row_items<OffT>(v, r.fbeg, r.fbeg + d, d, r.fdeg, small_cap, big_chunk, item_len, ctr,
+    post_row_items<OffT>(v, r.fbeg, r.fbeg + d, d, r.fdeg, small_cap, big_chunk, item_shift, ctr,
                          bitem, irow);
 }
 
@@ -550,7 +621,7 @@ template <typename OffT, int GS>
 __global__ void __launch_bounds__(256)
 row_place_kernel(const OffT *__restrict__ off, const int *__restrict__ ind, long long n,
                  int *__restrict__ deg, int *__restrict__ fcnt, int *__restrict__ find,
-                 VInfo *__restrict__ vinfo, int small_cap, int big_chunk, long long item_len,
+                 VInfo *__restrict__ vinfo, int small_cap, int big_chunk, int item_shift,
                  Counters *ctr, int2 *__restrict__ bitem, long long *__restrict__ irow,
                  unsigned int *status)
 {
@@ -586,7 +657,8 @@ row_place_kernel(const OffT *__restrict__ off, const int *__restrict__ ind, long
         r.fdeg = wrote;
         r.key = dv;
         vinfo[v] = r;
-        post_row_items<OffT>(v, b, e, dv, wrote, small_cap, big_chunk, item_len, ctr, bitem, irow);
+        post_row_items<OffT>(v, b, e, dv, wrote, small_cap, big_chunk, item_shift, ctr, bitem,
+                             irow);
     }
 }
 
@@ -1136,7 +1208,8 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
                  const int *__restrict__ find,
                  unsigned long long *__restrict__ tacc, Counters *ctr,
                  unsigned int *status, const int2 *__restrict__ bitem, int big_chunk,
-                 int big_hash_max, int small_cap, const int *__restrict__ order)
+                 int big_hash_max, int small_cap, const int *__restrict__ order,
+                 const int *__restrict__ rank_end)
 {
     extern __shared__ int smem[];
     int *keys = smem;
@@ -1175,7 +1248,9 @@ count_big_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
             if (lane == 0) st = atomicAdd(&s_next, 1);
             return rb + 32ll * warp.shfl(st, 0);
         };
-        const long long range = RANK ? n - 1 - (long long)ka : 0;
+        // N+(a) and every partner list lie in (ka, end): end = n, or with a
+        // batch's graph-major ranks the end of the apex's own graph's ranks
+        const long long range = RANK ? (rank_end ? (long long)rank_end[a] : n) - 1 - ka : n;
         if (RANK && range <= kDirectRanks) {
             // one 16-bit counter per rank above the apex; 0xffff marks a
             // rank outside N+(a), so the counter is also the membership test
@@ -1431,10 +1506,11 @@ gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
             return GTC_ERR_INVALID_ARGUMENT;
         cfg.group = tuning->group;
     }
-    // item_len and big_chunk bound the 16-bit shared hit counters: a counter
-    // collects at most one hit per adjacency entry of one work item
+    // item_len (a power of two) and big_chunk bound the 16-bit shared hit
+    // counters: a counter collects at most one hit per adjacency entry of one
+    // work item
     if (tuning->item_len < 0 || (tuning->item_len > 0 && tuning->item_len < kMinItemLen) ||
-        tuning->item_len > kMaxItemLen ||
+        tuning->item_len > kMaxItemLen || (tuning->item_len & (tuning->item_len - 1)) ||
         tuning->big_chunk < 0 || (tuning->big_chunk > 0 && tuning->big_chunk < kMinBigChunk) ||
         tuning->big_hash_max < 0 ||
         tuning->big_hash_max > kBigHashMaxFdeg || tuning->big_chunk > 32768 ||
@@ -1463,7 +1539,8 @@ template <typename OffT>
 gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz,
                      bool per_vertex, long long *r, long long *t, double *lcc,
                      long long *global, void *ws, size_t ws_bytes,
-                     cudaStream_t stream, const RowConfig &cfg, CountTimings *timing)
+                     cudaStream_t stream, const RowConfig &cfg, CountTimings *timing,
+                     const SegRanks *seg)
 {
     const int off_bits = sizeof(OffT) * 8;
     Plan p = make_plan(n, nnz, off_bits, per_vertex);
@@ -1501,10 +1578,23 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
         nvtxRangePushA("gtc: forward lists");
         const int small_cap = 4 * cfg.group;   // <= kRowSlots / 8
         if (rank_labels) {
-            const unsigned rb = (unsigned)div_up<long long>(n, kRankChunk);
-            degree_hist_kernel<<<rb, kRankThreads, 0, stream>>>(off, off_bits, n, deg, hist);
-            rank_scan_kernel<<<1, kRankScanThreads, 0, stream>>>(hist);
-            rank_kernel<<<rb, kRankThreads, 0, stream>>>(deg, n, hist, rank, order);
+            if (seg && seg->num_graphs > 0) {
+                const long long nb = seg->num_graphs * kSegBuckets;
+                unsigned long long *gh = reinterpret_cast<unsigned long long *>(seg->ghist);
+                err = cudaMemsetAsync(gh, 0, sizeof(long long) * (size_t)(nb + 1), stream);
+                if (err != cudaSuccess) return GTC_ERR_CUDA;
+                seg_degree_hist_kernel<OffT><<<vb, 256, 0, stream>>>(off, n, seg->vstart,
+                                                                     seg->num_graphs, deg, gh);
+                err = exclusive_scan_i64(seg->ghist, seg->ghist, nb, seg->scan_tmp, stream);
+                if (err != cudaSuccess) return GTC_ERR_CUDA;
+                seg_rank_kernel<<<vb, 256, 0, stream>>>(deg, n, seg->vstart, seg->num_graphs, gh,
+                                                        rank, order, seg->rank_end);
+            } else {
+                const unsigned rb = (unsigned)div_up<long long>(n, kRankChunk);
+                degree_hist_kernel<<<rb, kRankThreads, 0, stream>>>(off, off_bits, n, deg, hist);
+                rank_scan_kernel<<<1, kRankScanThreads, 0, stream>>>(hist);
+                rank_kernel<<<rb, kRankThreads, 0, stream>>>(deg, n, hist, rank, order);
+            }
             tile_bounds_kernel<OffT><<<(unsigned)div_up<long long>(p.n_tiles + 1, 256), 256, 0,
                                        stream>>>(off, n, nnz, p.n_tiles, trow, fcnt);
             tile_place_kernel<OffT, true><<<(unsigned)p.n_tiles, kPrepThreads, 0, stream>>>(
@@ -1518,8 +1608,8 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
             sort_lists_kernel<OffT><<<(unsigned)sb, kSortThreads, 0, stream>>>(
                 off, fcnt, n, find, ctr, min(4 * cfg.group, 31));
             vinfo_kernel<OffT><<<vb, 256, 0, stream>>>(off, fcnt, deg, rank, n, small_cap,
-                                                       cfg.big_chunk, cfg.item_len, vinfo, ctr,
-                                                       bitem, irow);
+                                                       cfg.big_chunk, ceil_log2(cfg.item_len),
+                                                       vinfo, ctr, bitem, irow);
         } else {
             // one row per group of gs lanes, gs ~ the mean degree
             const double mean = (double)nnz / (double)n;
@@ -1527,8 +1617,8 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
             const unsigned pb = (unsigned)div_up<long long>(n * gs, 256);
             auto place = [&](auto kern) {
                 kern<<<pb, 256, 0, stream>>>(off, ind, n, deg, fcnt, find, vinfo, small_cap,
-                                             cfg.big_chunk, cfg.item_len, ctr, bitem, irow,
-                                             status);
+                                             cfg.big_chunk, ceil_log2(cfg.item_len), ctr, bitem,
+                                             irow, status);
             };
             if (gs == 8) place(row_place_kernel<OffT, 8>);
             else if (gs == 16) place(row_place_kernel<OffT, 16>);
@@ -1537,6 +1627,7 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
         nvtxRangePop();
         if (timing) cudaEventRecord(timing->ev[1], stream);
         const int *lorder = rank_labels ? order : nullptr;
+        const int *rank_end = (rank_labels && seg && seg->num_graphs > 0) ? seg->rank_end : nullptr;
         if (nnz > 0) {
             const long long n_items = div_up<long long>(nnz, cfg.item_len);
             auto launch_rows = [&](auto kern) {
@@ -1561,7 +1652,8 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                 int blocks = occupancy_blocks(kern, kBigThreads, big_smem, dev, cache);
                 kern<<<blocks, kBigThreads, big_smem, stream>>>(off, ind, n, vinfo, find, tacc, ctr,
                                                                 status, bitem, cfg.big_chunk,
-                                                                cfg.big_hash_max, small_cap, lorder);
+                                                                cfg.big_hash_max, small_cap, lorder,
+                                                                rank_end);
             };
             int *bc = g_big_blocks[dev & 63];
             NvtxRange r("gtc: block kernel");
@@ -1587,10 +1679,11 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
 
 template gtc_status run_count<int>(const int *, const int *, long long, long long, bool,
                                    long long *, long long *, double *, long long *, void *,
-                                   size_t, cudaStream_t, const RowConfig &, CountTimings *);
+                                   size_t, cudaStream_t, const RowConfig &, CountTimings *,
+                                   const SegRanks *);
 template gtc_status run_count<long long>(const long long *, const int *, long long, long long,
                                          bool, long long *, long long *, double *, long long *,
                                          void *, size_t, cudaStream_t, const RowConfig &,
-                                         CountTimings *);
+                                         CountTimings *, const SegRanks *);
 
 }  // namespace gtc

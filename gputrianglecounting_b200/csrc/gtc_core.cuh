@@ -32,6 +32,20 @@ struct CountTimings {
     cudaEvent_t ev[5];
 };
 
+// Degree-rank labels for a batch: the vertex space is cut into graphs
+// (vstart[0..G]) and ranks are made graph-major -- graph g's vertices take the
+// ranks vstart[g] .. vstart[g+1]-1 in ascending degree order -- so that an
+// apex's forward list spans only its own graph's ranks.  ghist holds
+// G * kSegBuckets + 1 int64 counters, scan_tmp scan_tmp_bytes(G * kSegBuckets),
+// rank_end n ints (the end of each vertex's graph's ranks).
+struct SegRanks {
+    const long long *vstart = nullptr;
+    long long num_graphs = 0;
+    long long *ghist = nullptr;
+    void *scan_tmp = nullptr;
+    int *rank_end = nullptr;
+};
+
 Plan make_plan(long long n, long long nnz, int off_bits, bool per_vertex);
 RowConfig pick_row_config(long long n, long long nnz);
 
@@ -40,6 +54,6 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                      bool per_vertex, long long *r, long long *t, double *lcc,
                      long long *global, void *ws, size_t ws_bytes,
                      cudaStream_t stream, const RowConfig &cfg,
-                     CountTimings *timing);
+                     CountTimings *timing, const SegRanks *seg = nullptr);
 
 }  // namespace gtc

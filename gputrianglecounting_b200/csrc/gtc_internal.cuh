@@ -39,7 +39,7 @@ constexpr int kRowThreads = 256;            // warp-per-item count kernel
 constexpr int kRowSlots = 512;              // shared table slots per warp
 constexpr int kRowMinBlocks = 6;            // 48 warps per SM (register budget 42)
 constexpr int kMinItemLen = 32;             // smallest warp work item (entries)
-constexpr int kMaxItemLen = 65535;          // largest: a 16-bit hit counter must not carry
+constexpr int kMaxItemLen = 32768;          // largest: a 16-bit hit counter must not carry
 constexpr int kBigThreads = 256;            // block-per-row count kernel
 constexpr int kBigMinBlocks = 8;            // 8 blocks (64 warps) per SM: 32 registers
 constexpr int kMinBigChunk = 32;            // smallest block-kernel item (entries)
@@ -61,6 +61,7 @@ constexpr int kDirectRanks = 12288;         // block kernel: one 16-bit counter 
 constexpr int kTrimLoads = 4;               // block kernel: loads in flight per partner window
 constexpr int kBitWords = 2048;             // block kernel rank bitmap: 65536 ranks
 constexpr int kBitKeys = 2048;              // longest apex list on the bitmap path
+constexpr int kSegBuckets = 1024;           // degree buckets per graph (batched rank labels)
 
 // Error bits written to the workspace status word (the first 4 bytes of
 // every counting workspace) by device code; gtc_count_status reads them.
@@ -141,5 +142,12 @@ struct Counters {
     unsigned long long pad[2];
 };
 
+
+// out[0..count) = exclusive prefix of in, out[count] = total (in may be out);
+// tmp holds scan_tmp_bytes(count) bytes.
+size_t scan_tmp_bytes(long long count);
+cudaError_t exclusive_scan_i64(const long long *in, long long *out,
+                               long long count, void *tmp,
+                               cudaStream_t stream);
 
 }  // namespace gtc

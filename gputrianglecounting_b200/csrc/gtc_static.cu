@@ -12,8 +12,9 @@
 // Limits and rules:
 //   * the array holds kStaticScratchBytes (32 MiB); a graph whose workspace
 //     (gtc_workspace_size) is larger is rejected with GTC_ERR_CAPACITY before
-//     any device work -- about 52 bytes per vertex plus 4 bytes per adjacency
-//     entry plus 64 KiB, e.g. 100,000 vertices with 4 million entries fit;
+//     any device work -- about 48 bytes per vertex plus 4.5 bytes per
+//     adjacency entry plus 67 KiB, e.g. 100,000 vertices with 4 million
+//     entries fit;
 //   * every device that loads the library holds the array until the process
 //     exits;
 //   * the array is shared by all calls on a device and keeps the last call's

@@ -119,7 +119,7 @@ gtc_status gtc_count_status(const void *d_workspace, size_t ws_bytes,
  *   group        lanes that share one apex row in the group kernel: 4, 8,
  *                16 or 32; rows whose forward list is longer than
  *                4*group go to the block kernel
- *   item_len     adjacency entries per warp work item (32 .. 65535)
+ *   item_len     adjacency entries per warp work item (a power of two, 32 .. 32768)
  *   big_chunk    adjacency entries per block-kernel work item (32 .. 32768)
  *   big_hash_max longest forward list the block kernel hashes in shared
  *                memory (<= 2048); longer lists are binary-searched in place
@@ -162,13 +162,14 @@ gtc_status gtc_count_tuned(const void *d_off, int off_bits,
  * Diagnostic: one synchronous per-vertex count on the legacy default stream
  * with CUDA events between the pipeline phases; writes the device time in ms
  * of {forward-list build, group kernel, block kernel, epilogue} to h_ms[4].
- * Stands in for the reference's chrono timing around launch + sync
- * (src/gpurun.cu:17-47, timedKernelCall :469-508).
+ * tuning: as for gtc_count_tuned (NULL = the library's choice).  Stands in for
+ * the reference's chrono timing around launch + sync (src/gpurun.cu:17-47,
+ * timedKernelCall :469-508).
  */
 gtc_status gtc_count_phase_times(const void *d_off, int off_bits,
                                  const int32_t *d_ind, int64_t n, int64_t nnz,
                                  void *d_workspace, size_t ws_bytes,
-                                 float *h_ms);
+                                 float *h_ms, const gtc_tuning *tuning);
 
 /*
  * gtc_count with no device allocation at all, for callers that cannot

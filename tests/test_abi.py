@@ -88,15 +88,17 @@ def test_invalid_arguments_rejected_before_any_device_work():
     bad = _lib.Tuning(labels=5)
     assert lib.gtc_count_tuned(fake, 32, fake, 10, 4, 0, None, None, None, None, fake, 1 << 20,
                                None, ctypes.byref(bad)) == 1
-    # item_len above 65535 could carry a 16-bit shared hit counter into its
-    # neighbour; rejected (host-only check, also in the launch plan)
+    # item_len above 32768 could carry a 16-bit shared hit counter into its
+    # neighbour, and it must be a power of two; rejected (host-only check,
+    # also in the launch plan)
     bad = _lib.Tuning(item_len=65536)
     assert lib.gtc_count_tuned(fake, 32, fake, 10, 4, 0, None, None, None, None, fake, 1 << 20,
                                None, ctypes.byref(bad)) == 1
     from gputrianglecounting_b200 import api
-    assert api.launch_plan(1000, 90000, tuning={"item_len": 65535})["launches"] > 0
-    with pytest.raises(_lib.GTCError):
-        api.launch_plan(1000, 90000, tuning={"item_len": 65536})
+    assert api.launch_plan(1000, 90000, tuning={"item_len": 32768})["launches"] > 0
+    for bad_len in (65536, 65535, 48, 100):
+        with pytest.raises(_lib.GTCError):
+            api.launch_plan(1000, 90000, tuning={"item_len": bad_len})
     # status query needs a workspace
     assert lib.gtc_count_status(None, 256, None, None) == 1
     assert lib.gtc_count_status(fake, 2, None, None) == 1

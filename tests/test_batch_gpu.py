@@ -37,7 +37,9 @@ def test_batch_matches_oracle_and_single_graph(cuda):
     graphs = _mixed_graphs()
     batch = G.concat_graphs(graphs, cuda)
     bc = api.BatchCounter(cuda)
-    for tun in (None, {"group": 4}, {"group": 32, "item_len": 64, "big_chunk": 64}):
+    for tun in (None, {"group": 4}, {"group": 32, "item_len": 64, "big_chunk": 64},
+                {"labels": 2}, {"labels": 2, "group": 4, "big_chunk": 64},
+                {"labels": 1, "group": 4, "big_hash_max": 8}):
         res = bc.count(batch, outputs=("r", "lcc", "graph_T"), tuning=tun)
         torch.cuda.synchronize()
         _check_against_oracle(graphs, batch, res)
@@ -131,11 +133,9 @@ def test_full_batched_workload_per_vertex_equals_single_graph(cuda):
     graphs = [G.make_spec_graph(s, cuda) for s in specs]
     batch = G.concat_graphs(graphs, cuda)
     bc = api.BatchCounter(cuda)
-    res = bc.count(batch, outputs=("r", "lcc", "graph_T"))
-    bc.check_status()
     tc = api.TriangleCounter(cuda)
-    r_one = torch.empty_like(res.r)
-    lcc_one = torch.empty_like(res.lcc)
+    r_one = torch.empty(batch.total_n, dtype=torch.int64, device=cuda)
+    lcc_one = torch.empty(batch.total_n, dtype=torch.float64, device=cuda)
     T_one = torch.empty(len(graphs), 3, dtype=torch.int64, device=cuda)
     vstart = batch.vstart.cpu().numpy()
     for i, g in enumerate(graphs):
@@ -143,6 +143,11 @@ def test_full_batched_workload_per_vertex_equals_single_graph(cuda):
         tc.count(g.off, g.ind, out=api.TriangleCounts(r=r_one[sl], t=None, lcc=lcc_one[sl],
                                                       global_counts=T_one[i]))
     torch.cuda.synchronize()
-    assert torch.equal(res.r, r_one)
-    assert torch.equal(res.lcc.view(torch.int64), lcc_one.view(torch.int64))
-    assert torch.equal(res.graph_T, T_one[:, 0])
+    # vertex-id labels (the library's choice for this mean degree) and
+    # graph-major degree ranks
+    for tun in (None, {"labels": 2, "group": 16}):
+        res = bc.count(batch, outputs=("r", "lcc", "graph_T"), tuning=tun)
+        bc.check_status()
+        assert torch.equal(res.r, r_one), tun
+        assert torch.equal(res.lcc.view(torch.int64), lcc_one.view(torch.int64)), tun
+        assert torch.equal(res.graph_T, T_one[:, 0]), tun
