@@ -50,6 +50,10 @@ CONFIGS = {
                           "from the batched-workload generator (pool of 256, seed 5) or, with "
                           "probability 1%, an R-MAT scale 22 edge factor 16 graph; CSRs resident "
                           "in HBM"),
+    "ops": dict(kind="ops", pool=256, seed=5, vertices=1 << 16,
+                label="the reference-compatible operators on R-MAT scale 20 (kernelCall with int64 "
+                      "ids, its vertex-list overload on 65,536 vertices, CSR validation) and the "
+                      "pack + batched count of a 256-graph pool of the batched generator (seed 5)"),
     "batched": dict(kind="batched", graphs=4096, seed=4,
                     label="4,096 graphs, n log-uniform in [256, 262144], half ER (mean degree "
                           "U[8,32]), half R-MAT (0.57,0.19,0.19,0.05, edge factor U[8,16]), seed 4; "
@@ -306,6 +310,8 @@ def run_reference(args, cfg, rank: int) -> None:
     if cfg["kind"] in ("batched", "serving"):
         run_reference_batched(args, CONFIGS["batched"], threads)
         return
+    if cfg["kind"] == "ops":                # the operators' graph: R-MAT scale 20
+        cfg = CONFIGS["rmat20"]
     g = int32_offsets(make_graph(cfg, "cpu").numpy())
     rt = ReferenceTimer(g, threads)
     t0 = time.perf_counter()
@@ -512,7 +518,8 @@ def run_b200(args, name: str, rank: int, world: int, with_baseline: bool = True)
 
 def launches_per_count(n: int, nnz: int, tuning: dict | None = None) -> int:
     """Kernels of one plain count with every output (the library's own plan:
-    5 with vertex-id labels, 11 with degree-rank labels)."""
+    5 with vertex-id labels, 6 from 2^18 rows on, 11 with degree-rank
+    labels)."""
     from gputrianglecounting_b200 import api
     return api.launch_plan(n, nnz, tuning=tuning)["launches"]
 
@@ -689,6 +696,63 @@ def run_batched(args, cfg, rank: int, world: int):
 
 # ------------------------------------------------------------------ serving
 
+def run_ops(args, cfg, rank: int, world: int):
+    """Device time per call of the library's other operators: the reference's
+    kernelCall<int64_t> argument list on the whole R-MAT 20 graph (int64 ids
+    narrowed on the device), its vertex-list overload on 65,536 seeded
+    vertices, CSR validation, and gtc_batch_pack + gtc_count_batch of a pool
+    of 256 device-resident graphs."""
+    import torch
+    from gputrianglecounting_b200 import api, graphs as G
+    from gputrianglecounting_b200._lib import load as load_lib
+    load_lib()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    host = int32_offsets(make_graph(CONFIGS["rmat20"], "cpu").numpy())
+    off = torch.from_numpy(host.off).to(dev)
+    ind = torch.from_numpy(host.ind).to(dev)
+    off64, ind64 = off.to(torch.int64), ind.to(torch.int64)
+    out64 = torch.empty(host.n, dtype=torch.int64, device=dev)
+    rng = np.random.default_rng(cfg["seed"])
+    verts = torch.from_numpy(rng.integers(0, host.n, cfg["vertices"]).astype(np.int64)).to(dev)
+    vout = torch.empty(cfg["vertices"], dtype=torch.int64, device=dev)
+    pool = [G.make_spec_graph(s, dev) for s in G.batched_specs(cfg["pool"], cfg["seed"])]
+    bc = api.BatchCounter(dev)
+    tun = {"group": 16, "labels": 2, "region": 4, "big_chunk": 4096, "item_len": 1024}
+    ops = {
+        "kernelCall_i64": lambda: api.kernelCall(1, 256, host.n, off64, ind64, out64, 1, 256, 0),
+        "kernelCall_vertex_i64": lambda: api.kernelCall(1, 256, cfg["vertices"], off64, ind64, vout,
+                                                       1, 256, 0, vertex=verts),
+        "validate_csr": lambda: api.validate_csr(off, ind),
+        "batch_pack_and_count": lambda: bc.count(bc.pack(pool), tuning=tun),
+    }
+    res = {}
+    for name, fn in ops.items():
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        res[name] = {"ms": statistics.mean(ms), "ms_min": min(ms)}
+    if rank != 0:
+        return None
+    pool_m = sum(g.nnz for g in pool) // 2
+    return {"metric": "operator device time per call", "value": res["kernelCall_i64"]["ms"],
+            "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["kernelCall_i64"]["ms"], "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE, "data": "synthetic",
+            "config": {"workload": "ops", "graph": cfg["label"], "n": host.n, "nnz": host.nnz,
+                       "pool_graphs": len(pool), "pool_m": pool_m},
+            "ops": res}
+
+
 def run_serving(args, cfg, rank: int, world: int):
     """Continuous batching under Poisson load: p50/p99 latency and sustained
     edges/s per arrival rate (each rank serves its own stream)."""
@@ -777,6 +841,8 @@ def main() -> None:
     try:
         if args.config == "batched":
             line = run_batched(args, cfg, rank, world)
+        elif args.config == "ops":
+            line = run_ops(args, cfg, rank, world)
         elif args.config == "serving":
             line = run_serving(args, cfg, rank, world)
         else:

@@ -4,6 +4,7 @@
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
 
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -57,11 +58,14 @@ __global__ void validate_rows_kernel(const OffT *__restrict__ off,
     }
 }
 
-// Phase 3 (warp per row): every (a, x) has its mirror (x, a).
+// Phase 3: every (a, x) has its mirror (x, a).  Warps take 32-entry strides
+// of the adjacency (so a hub row is spread over many warps); each lane finds
+// its entry's row from the stride's first row.
 template <typename OffT>
 __global__ void validate_symmetry_kernel(const OffT *__restrict__ off,
                                          const int *__restrict__ ind, long long n,
-                                         int *reason, unsigned long long *counts)
+                                         long long nnz, int *reason,
+                                         unsigned long long *counts)
 {
     // Rows are strictly ascending without self-loops (checked before), so
     // reversal maps the entries (a, x) with a < x injectively onto those with
@@ -72,25 +76,30 @@ __global__ void validate_symmetry_kernel(const OffT *__restrict__ off,
     const int lane = threadIdx.x & 31;
     const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
     unsigned long long upper = 0, lower = 0;
-    for (long long a = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < n; a += warps) {
-        const long long rb = off[a], re = off[a + 1];
-        bool ok = true;
-        for (long long e = rb + lane; e < re; e += 32) {
+    bool ok = true;
+    for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 < nnz;
+         w += warps) {
+        const long long e = w * 32 + lane;
+        long long a = 0;
+        if (lane == 0) a = row_of_entry(off, n, w * 32);
+        a = __shfl_sync(0xffffffffu, a, 0);
+        if (e < nnz) {
+            while ((long long)off[a + 1] <= e) ++a;
             const int x = ind[e];
             if (x < a) {
                 ++lower;
-                continue;
+            } else {
+                ++upper;
+                long long lo = off[x], hi = off[x + 1];
+                while (lo < hi) {
+                    const long long mid = (lo + hi) >> 1;
+                    if (ind[mid] < a) lo = mid + 1; else hi = mid;
+                }
+                if (lo >= (long long)off[x + 1] || ind[lo] != a) ok = false;
             }
-            ++upper;
-            long long lo = off[x], hi = off[x + 1];
-            while (lo < hi) {
-                long long mid = (lo + hi) >> 1;
-                if (ind[mid] < a) lo = mid + 1; else hi = mid;
-            }
-            if (lo >= (long long)off[x + 1] || ind[lo] != a) ok = false;
         }
-        if (!__all_sync(0xffffffffu, ok) && lane == 0) atomicMin(reason, GTC_CSR_ASYMMETRIC);
     }
+    if (!__all_sync(0xffffffffu, ok) && lane == 0) atomicMin(reason, GTC_CSR_ASYMMETRIC);
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
         upper += __shfl_down_sync(0xffffffffu, upper, d);
@@ -122,7 +131,13 @@ gtc_status run_validate(const OffT *off, const int *ind, long long n, long long 
         long long want = div_up<long long>(n, 8);
         unsigned blocks = (unsigned)(want < (long long)sms * 16 ? want : (long long)sms * 16);
         validate_rows_kernel<<<blocks, 256, 0, stream>>>(off, ind, n, reason);
-        validate_symmetry_kernel<<<blocks, 256, 0, stream>>>(off, ind, n, reason, counts);
+        if (nnz > 0) {
+            const long long swant = div_up<long long>(nnz, 32 * 8);
+            const unsigned sblocks =
+                (unsigned)(swant < (long long)sms * 16 ? swant : (long long)sms * 16);
+            validate_symmetry_kernel<<<sblocks, 256, 0, stream>>>(off, ind, n, nnz, reason,
+                                                                  counts);
+        }
     }
     // reason word and the two entry counts in one read
     unsigned char host[80];
@@ -143,6 +158,9 @@ gtc_status run_validate(const OffT *off, const int *ind, long long n, long long 
 
 constexpr int kSubThreads = 256;
 constexpr int kSubSlots = 4096;
+constexpr long long kSubHubMin = kSubSlots / 2;   // longer listed rows go to the hub kernel
+constexpr int kSubHubThreads = 1024;
+constexpr long long kSubHubBits = 1ll << 20;      // bitmap span of a hub row (128 KiB)
 
 template <typename IndT>
 __device__ __forceinline__ bool sorted_contains(const IndT *__restrict__ list,
@@ -156,13 +174,50 @@ __device__ __forceinline__ bool sorted_contains(const IndT *__restrict__ list,
     return lo < len && (long long)list[lo] == key;
 }
 
+// |N(u) ∩ N(v)| by binary search of the shorter sorted row in the longer,
+// this lane's share (lane stride 32).
+template <typename IndT>
+__device__ __forceinline__ unsigned long long search_shorter(const IndT *__restrict__ ind,
+                                                             long long vb, long long dv,
+                                                             long long ub, long long du,
+                                                             int lane)
+{
+    unsigned long long acc = 0;
+    if (du < dv) {
+        for (long long i = lane; i < du; i += 32)
+            acc += sorted_contains(ind + vb, dv, (long long)ind[ub + i]);
+    } else {
+        for (long long i = lane; i < dv; i += 32)
+            acc += sorted_contains(ind + ub, du, (long long)ind[vb + i]);
+    }
+    return acc;
+}
+
+__device__ __forceinline__ void add_out(long long *o, unsigned long long x)
+{
+    atomicAdd(reinterpret_cast<unsigned long long *>(o), x);
+}
+__device__ __forceinline__ void add_out(int *o, unsigned long long x)
+{
+    atomicAdd(o, (int)x);
+}
+
 // out[k] = sum over u in N(v) of |N(v) ∩ N(u)|, v = vertex[k], with full
 // adjacency lists (the rows of the listed vertices and of their neighbours
 // are the only ones read, as in the reference's vertex-list kernel,
-// src/clusteringCount.cu:266-312).  Block per listed vertex: N(v) goes to a
-// shared hash table; for each neighbour u the shorter side is probed (N(u)
-// into the table, or N(v) by binary search into N(u)).  Edges with u == v
-// or a list shorter than two are skipped like the reference (:292-294).
+// src/clusteringCount.cu:266-312).  Edges with u == v or a list shorter
+// than two are skipped like the reference (:292-294).  Two kernels:
+//   * subset_kernel, a block per listed vertex of degree <= kSubHubMin: N(v)
+//     goes to a shared hash table; for each neighbour u, N(u) is probed into
+//     the table when it is not much longer, otherwise the shorter row is
+//     binary-searched in the longer.  It writes 0 for the longer rows;
+//   * subset_hub_kernel, all blocks on every longer ("hub") row: each block
+//     sets N(v) in a shared bitmap over the row's id span and takes every
+//     gridDim.x-th neighbour, whose row its warps probe into the bitmap with
+//     coalesced loads; block sums are added to out[k].  A row whose span
+//     exceeds the bitmap falls back to the binary search.
+// Spreading a hub over the whole GPU matters: on a power-law graph a single
+// hub's probes outnumber those of thousands of ordinary rows.
 template <typename OffT, typename IndT, typename VtxT, typename OutT>
 __global__ void __launch_bounds__(kSubThreads)
 subset_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
@@ -178,24 +233,25 @@ subset_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
     for (long long k = blockIdx.x; k < count; k += gridDim.x) {
         const long long v = (long long)vertex[k];
         const long long vb = off[v], ve = off[v + 1], dv = ve - vb;
+        if (dv > kSubHubMin) {
+            if (threadIdx.x == 0) out[k] = 0;
+            continue;                              // uniform across the block
+        }
         if (threadIdx.x == 0) s_sum = 0;
-        const bool use_table = dv <= kSubSlots / 2;
         int log2t = 5;
         while ((1ll << log2t) < 2 * dv) ++log2t;
         const unsigned int mask = (1u << log2t) - 1;
-        if (use_table) {
-            for (int i = threadIdx.x; i <= (int)mask; i += kSubThreads) s_keys[i] = -1;
-            __syncthreads();
-            for (long long i = threadIdx.x; i < dv; i += kSubThreads) {
-                const long long key = (long long)ind[vb + i];
-                unsigned int slot = hash_slot((int)key, log2t);
-                while (true) {
-                    unsigned long long prev = atomicCAS((unsigned long long *)&s_keys[slot],
-                                                        (unsigned long long)-1ll,
-                                                        (unsigned long long)key);
-                    if (prev == (unsigned long long)-1ll) break;
-                    slot = (slot + 1) & mask;
-                }
+        for (int i = threadIdx.x; i <= (int)mask; i += kSubThreads) s_keys[i] = -1;
+        __syncthreads();
+        for (long long i = threadIdx.x; i < dv; i += kSubThreads) {
+            const long long key = (long long)ind[vb + i];
+            unsigned int slot = hash_slot((int)key, log2t);
+            while (true) {
+                unsigned long long prev = atomicCAS((unsigned long long *)&s_keys[slot],
+                                                    (unsigned long long)-1ll,
+                                                    (unsigned long long)key);
+                if (prev == (unsigned long long)-1ll) break;
+                slot = (slot + 1) & mask;
             }
         }
         __syncthreads();
@@ -206,7 +262,7 @@ subset_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
                 const long long u = (long long)ind[e];
                 const long long ub = off[u], ue = off[u + 1], du = ue - ub;
                 if (u == v || du < 2) continue;
-                if (use_table && du <= 4 * dv) {
+                if (du <= 4 * dv) {
                     for (long long i = lane; i < du; i += 32) {
                         const long long w = (long long)ind[ub + i];
                         unsigned int slot = hash_slot((int)w, log2t);
@@ -218,10 +274,7 @@ subset_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
                         }
                     }
                 } else {
-                    for (long long i = lane; i < dv; i += 32) {
-                        const long long w = (long long)ind[vb + i];
-                        acc += sorted_contains(ind + ub, du, w);
-                    }
+                    acc += search_shorter(ind, vb, dv, ub, du, lane);
                 }
             }
         }
@@ -230,6 +283,100 @@ subset_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
         __syncthreads();
         if (threadIdx.x == 0) out[k] = (OutT)s_sum;
         __syncthreads();
+    }
+}
+
+template <typename OffT, typename IndT, typename VtxT, typename OutT>
+__global__ void __launch_bounds__(kSubHubThreads, 1)
+subset_hub_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
+                  const VtxT *__restrict__ vertex, long long count,
+                  OutT *__restrict__ out)
+{
+    extern __shared__ unsigned int s_bits[];          // kSubHubBits / 32 words
+    __shared__ long long s_hub[kSubHubThreads];
+    __shared__ int s_nhub;
+    __shared__ long long s_lo, s_hi;
+    __shared__ unsigned long long s_sum;
+    auto block = cg::this_thread_block();
+    auto warp = cg::tiled_partition<32>(block);
+    const int wid = warp.meta_group_rank(), lane = warp.thread_rank();
+    constexpr int nwarps = kSubHubThreads / 32;
+    const long long stride = (long long)gridDim.x * nwarps;   // neighbours per worker step
+    // the listed vertices are scanned a chunk at a time, every thread
+    // testing one; the hubs found are then taken one after another
+    for (long long c0 = 0; c0 < count; c0 += kSubHubThreads) {
+        if (threadIdx.x == 0) s_nhub = 0;
+        __syncthreads();
+        const long long kk = c0 + threadIdx.x;
+        if (kk < count) {
+            const long long v = (long long)vertex[kk];
+            if ((long long)off[v + 1] - (long long)off[v] > kSubHubMin)
+                s_hub[atomicAdd(&s_nhub, 1)] = kk;
+        }
+        __syncthreads();
+        const int nh = s_nhub;
+        for (int h = 0; h < nh; ++h) {
+            const long long k = s_hub[h];
+            const long long v = (long long)vertex[k];
+            const long long vb = off[v], ve = off[v + 1], dv = ve - vb;
+            // the row's id span (rows are sorted, but the bitmap must not
+            // depend on it)
+            long long lo = LLONG_MAX, hi = LLONG_MIN;
+            for (long long i = vb + threadIdx.x; i < ve; i += kSubHubThreads) {
+                const long long x = (long long)ind[i];
+                lo = min(lo, x);
+                hi = max(hi, x);
+            }
+            lo = cg::reduce(warp, lo, cg::less<long long>());
+            hi = cg::reduce(warp, hi, cg::greater<long long>());
+            if (threadIdx.x == 0) { s_lo = LLONG_MAX; s_hi = LLONG_MIN; s_sum = 0; }
+            __syncthreads();
+            if (lane == 0) { atomicMin(&s_lo, lo); atomicMax(&s_hi, hi); }
+            __syncthreads();
+            lo = s_lo;
+            hi = s_hi;
+            const unsigned long long span = (unsigned long long)(hi - lo) + 1ull;
+            const bool use_bits = span <= (unsigned long long)kSubHubBits;
+            if (use_bits) {
+                const int words = (int)((span + 31) >> 5);
+                for (int i = threadIdx.x; i < words; i += kSubHubThreads) s_bits[i] = 0;
+                __syncthreads();
+                for (long long i = vb + threadIdx.x; i < ve; i += kSubHubThreads) {
+                    const unsigned long long x = (unsigned long long)((long long)ind[i] - lo);
+                    atomicOr(&s_bits[x >> 5], 1u << (x & 31));
+                }
+                __syncthreads();
+            }
+            unsigned long long acc = 0;
+            for (long long e = vb + blockIdx.x + (long long)gridDim.x * wid; e < ve; e += stride) {
+                const long long u = (long long)ind[e];
+                const long long ub = off[u], ue = off[u + 1], du = ue - ub;
+                if (u == v || du < 2) continue;
+                if (use_bits) {
+                    // four loads in flight per lane
+                    for (long long i0 = ub; i0 < ue; i0 += 128) {
+                        long long x[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const long long i = i0 + j * 32 + lane;
+                            x[j] = i < ue ? (long long)ind[i] - lo : -1;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                            if ((unsigned long long)x[j] < span)
+                                acc += (s_bits[x[j] >> 5] >> (x[j] & 31)) & 1u;
+                    }
+                } else {
+                    acc += search_shorter(ind, vb, dv, ub, du, lane);
+                }
+            }
+            const unsigned long long ws = cg::reduce(warp, acc, cg::plus<unsigned long long>());
+            if (lane == 0 && ws) atomicAdd(&s_sum, ws);
+            __syncthreads();
+            if (threadIdx.x == 0 && s_sum) add_out(&out[k], s_sum);
+            __syncthreads();                       // s_bits, s_lo and s_sum are reused
+        }
+        __syncthreads();                           // every thread has read s_nhub
     }
 }
 
@@ -244,6 +391,14 @@ gtc_status launch_subset(const OffT *off, const IndT *ind, const VtxT *vertex,
     long long blocks = count < (long long)sms * 8 ? count : (long long)sms * 8;
     subset_kernel<OffT, IndT, VtxT, OutT><<<(unsigned)blocks, kSubThreads, 0, stream>>>(
         off, ind, vertex, count, out);
+    // the hub kernel adds to what subset_kernel wrote (0 for hubs), in
+    // stream order
+    auto hub = subset_hub_kernel<OffT, IndT, VtxT, OutT>;
+    const int smem = (int)(kSubHubBits / 8);
+    if (cudaFuncSetAttribute(hub, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        cudaSuccess)
+        return GTC_ERR_CUDA;
+    hub<<<(unsigned)sms, kSubHubThreads, smem, stream>>>(off, ind, vertex, count, out);
     return cudaGetLastError() == cudaSuccess ? GTC_OK : GTC_ERR_CUDA;
 }
 
@@ -367,7 +522,7 @@ gtc_status gtc_count_launches(int64_t n, int64_t nnz, gtc_mode mode,
     RowConfig cfg = pick_row_config(n, nnz);
     const gtc_status st = apply_tuning(cfg, tuning);
     if (st != GTC_OK) return st;
-    *launches = launches_per_count(cfg, mode == GTC_MODE_PLAIN);
+    *launches = launches_per_count(cfg, mode == GTC_MODE_PLAIN, n);
     *labels = cfg.rank_labels ? GTC_LABELS_DEGREE_RANK : GTC_LABELS_VERTEX_ID;
     return GTC_OK;
 }

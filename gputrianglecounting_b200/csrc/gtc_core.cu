@@ -610,13 +610,71 @@ __global__ void vinfo_kernel(const OffT *__restrict__ off, const int *__restrict
                          bitem, irow);
 }
 
-// Vertex-id labels: the whole forward build in one pass, a group of GS lanes
-// per row.  The group reads the row in GS-entry chunks, takes each
-// neighbour's degree from the offsets, keeps the entries ordered above the
-// row ((degree, id) order) and writes them, compacted by ballot, to the start
-// of the row's own CSR segment -- so every list keeps the row's ascending id
-// order and needs no sort.  The first lane then writes deg, fcnt, the
-// per-vertex record and the row's work items.
+// Vertex-id labels: the whole forward build in one pass.  Each row's entries
+// are read in chunks by a group of GS lanes, which takes each neighbour's
+// degree from the offsets, keeps the entries ordered above the row ((degree,
+// id) order) and writes them, compacted by ballot, to the start of the row's
+// own CSR segment -- so every list keeps the row's ascending id order and
+// needs no sort.  Then the row's deg, fcnt, per-vertex record and work items
+// are written.  Two launch forms:
+//   * row_place_kernel: one group per row, its first lane writing the row's
+//     records (small graphs: the most groups in flight);
+//   * row_place_warp_kernel: a warp per 32 consecutive rows; one lane per row
+//     loads the offsets and writes the records (coalesced) and the groups
+//     take the rows in turn; rows longer than max(8 x GS, kLongRowMin) are
+//     listed for long_row_place_kernel, a block per row, so that a hub holds
+//     up neither its warp's other rows nor a single group (large graphs).
+template <int GS>
+__device__ __forceinline__ int place_row(const int *__restrict__ ind, const void *offp,
+                                         bool off32, long long n, long long v, long long b,
+                                         int dv, int glane, int *__restrict__ find,
+                                         unsigned int *status)
+{
+    auto off_at = [&](long long i) -> long long {
+        return off32 ? (long long)static_cast<const int *>(offp)[i]
+                     : static_cast<const long long *>(offp)[i];
+    };
+    auto grp = cg::tiled_partition<GS>(cg::this_thread_block());
+    int wrote = 0;
+    for (int k0 = 0; k0 < dv; k0 += GS) {
+        const int k = k0 + glane;
+        bool fwd = false;
+        int x = 0;
+        if (k < dv) {
+            x = ind[b + k];
+            if ((unsigned long long)(long long)x < (unsigned long long)n) {
+                const int dx = (int)(off_at(x + 1) - off_at(x));
+                fwd = dx > dv || (dx == dv && x > v);
+            } else {
+                atomicOr(status, kErrIndexRange);
+            }
+        }
+        const unsigned int m = grp.ballot(fwd);
+        if (fwd) find[b + wrote + __popc(m & ((1u << glane) - 1u))] = x;
+        wrote += __popc(m);
+    }
+    return wrote;
+}
+
+template <typename OffT>
+__device__ __forceinline__ void row_records(const OffT *off, long long v, long long b,
+                                            long long e, int wrote, int small_cap,
+                                            int big_chunk, int item_shift, int *__restrict__ deg,
+                                            int *__restrict__ fcnt, VInfo *__restrict__ vinfo,
+                                            Counters *ctr, int2 *__restrict__ bitem,
+                                            long long *__restrict__ irow)
+{
+    const int d = (int)(e - b);
+    deg[v] = d;
+    fcnt[v] = wrote;
+    VInfo r;
+    r.fbeg = b;
+    r.fdeg = wrote;
+    r.key = d;
+    vinfo[v] = r;
+    post_row_items<OffT>(v, b, e, d, wrote, small_cap, big_chunk, item_shift, ctr, bitem, irow);
+}
+
 template <typename OffT, int GS>
 __global__ void __launch_bounds__(256)
 row_place_kernel(const OffT *__restrict__ off, const int *__restrict__ ind, long long n,
@@ -625,40 +683,123 @@ row_place_kernel(const OffT *__restrict__ off, const int *__restrict__ ind, long
                  Counters *ctr, int2 *__restrict__ bitem, long long *__restrict__ irow,
                  unsigned int *status)
 {
-    auto grp = cg::tiled_partition<GS>(cg::this_thread_block());
     const long long v = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / GS;
     if (v >= n) return;                      // uniform across the group
-    const int lane = grp.thread_rank();
+    const int glane = (threadIdx.x & 31) % GS;
     const long long b = (long long)off[v], e = (long long)off[v + 1];
-    const int dv = (int)(e - b);
-    int wrote = 0;
-    for (int k0 = 0; k0 < dv; k0 += GS) {
-        const int k = k0 + lane;
-        bool fwd = false;
-        int x = 0;
-        if (k < dv) {
-            x = ind[b + k];
-            if ((unsigned long long)(long long)x < (unsigned long long)n) {
-                const int dx = (int)((long long)off[x + 1] - (long long)off[x]);
-                fwd = dx > dv || (dx == dv && x > v);
-            } else {
-                atomicOr(status, kErrIndexRange);
-            }
-        }
-        const unsigned int m = grp.ballot(fwd);
-        if (fwd) find[b + wrote + __popc(m & ((1u << lane) - 1u))] = x;
-        wrote += __popc(m);
+    const int wrote = place_row<GS>(ind, off, sizeof(OffT) == 4, n, v, b, (int)(e - b), glane,
+                                    find, status);
+    if (glane == 0)
+        row_records<OffT>(off, v, b, e, wrote, small_cap, big_chunk, item_shift, deg, fcnt, vinfo,
+                          ctr, bitem, irow);
+}
+
+template <typename OffT, int GS>
+__global__ void __launch_bounds__(256)
+row_place_warp_kernel(const OffT *__restrict__ off, const int *__restrict__ ind, long long n,
+                      int *__restrict__ deg, int *__restrict__ fcnt, int *__restrict__ find,
+                      VInfo *__restrict__ vinfo, int small_cap, int big_chunk, int item_shift,
+                      Counters *ctr, int2 *__restrict__ bitem, long long *__restrict__ irow,
+                      int *__restrict__ long_rows, unsigned int *status)
+{
+    constexpr int kGroups = 32 / GS;
+    constexpr int kLong = 8 * GS > kLongRowMin ? 8 * GS : kLongRowMin;   // handed on beyond
+    const int lane = threadIdx.x & 31, glane = lane % GS, gi = lane / GS;
+    const long long v0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x - lane);
+    if (v0 >= n) return;                         // uniform across the warp
+    const long long my_v = v0 + lane;
+    const bool my_ok = my_v < n;
+    const long long my_b = my_ok ? (long long)off[my_v] : 0;
+    const long long my_e = my_ok ? (long long)off[my_v + 1] : 0;
+    const bool my_long = my_e - my_b > kLong;
+    int my_wrote = 0;
+#pragma unroll 1
+    for (int it = 0; it < 32 / kGroups; ++it) {
+        const int rl = it * kGroups + gi;            // this group's row (lane index)
+        const long long v = v0 + rl;
+        const long long b = __shfl_sync(0xffffffffu, my_b, rl);
+        const long long e = __shfl_sync(0xffffffffu, my_e, rl);
+        int wrote = 0;
+        if (v < n && e - b <= kLong)
+            wrote = place_row<GS>(ind, off, sizeof(OffT) == 4, n, v, b, (int)(e - b), glane, find,
+                                  status);
+        // row rl's count goes to lane rl
+        const int got = __shfl_sync(0xffffffffu, wrote, (lane % kGroups) * GS);
+        if (lane / kGroups == it) my_wrote = got;
     }
-    if (lane == 0) {
-        deg[v] = dv;
-        fcnt[v] = wrote;
-        VInfo r;
-        r.fbeg = b;
-        r.fdeg = wrote;
-        r.key = dv;
-        vinfo[v] = r;
-        post_row_items<OffT>(v, b, e, dv, wrote, small_cap, big_chunk, item_shift, ctr, bitem,
-                             irow);
+    if (my_ok && my_long) {
+        // long rows go to long_row_place_kernel, a block per row
+        const unsigned long long at = atomicAdd(&ctr->long_rows, 1ull);
+        long_rows[at] = (int)my_v;
+    } else if (my_ok) {
+        row_records<OffT>(off, my_v, my_b, my_e, my_wrote, small_cap, big_chunk, item_shift, deg,
+                          fcnt, vinfo, ctr, bitem, irow);
+    }
+}
+
+// The rows row_place_warp_kernel handed on (longer than its limit), a block
+// per row from a dynamic queue: the block's warps each take a contiguous
+// slice of the row, count their forward entries, place them after the
+// earlier slices' (a block scan of the counts), and the row's records follow.
+template <typename OffT>
+__global__ void __launch_bounds__(256)
+long_row_place_kernel(const OffT *__restrict__ off, const int *__restrict__ ind, long long n,
+                      int *__restrict__ deg, int *__restrict__ fcnt, int *__restrict__ find,
+                      VInfo *__restrict__ vinfo, int small_cap, int big_chunk, int item_shift,
+                      Counters *ctr, int2 *__restrict__ bitem, long long *__restrict__ irow,
+                      const int *__restrict__ long_rows, unsigned int *status)
+{
+    __shared__ long long s_idx;
+    __shared__ int s_cnt[8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const long long total = (long long)ctr->long_rows;
+    while (true) {
+        if (threadIdx.x == 0) s_idx = (long long)atomicAdd(&ctr->long_next, 1ull);
+        __syncthreads();
+        const long long idx = s_idx;
+        if (idx >= total) break;
+        const long long v = long_rows[idx];
+        const long long b = (long long)off[v], e = (long long)off[v + 1];
+        const int dv = (int)(e - b);
+        const int per = (dv + 7) / 8;
+        const int k_lo = min(wid * per, dv), k_hi = min(k_lo + per, dv);
+        // pass 1: forward entries of this warp's slice
+        auto fwd_at = [&](int k, int &x) -> bool {
+            x = ind[b + k];
+            if ((unsigned long long)(long long)x >= (unsigned long long)n) {
+                atomicOr(status, kErrIndexRange);
+                return false;
+            }
+            const int dx = (int)((long long)off[x + 1] - (long long)off[x]);
+            return dx > dv || (dx == dv && x > v);
+        };
+        int cnt = 0;
+        for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
+            const int k = k0 + lane;
+            int x = 0;
+            const bool f = k < k_hi && fwd_at(k, x);
+            cnt += __popc(__ballot_sync(0xffffffffu, f));
+        }
+        if (lane == 0) s_cnt[wid] = cnt;
+        __syncthreads();
+        int base = 0, wrote = 0;
+        for (int i = 0; i < 8; ++i) {
+            if (i < wid) base += s_cnt[i];
+            wrote += s_cnt[i];
+        }
+        // pass 2: place them, in row order
+        for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
+            const int k = k0 + lane;
+            int x = 0;
+            const bool f = k < k_hi && fwd_at(k, x);
+            const unsigned int m = __ballot_sync(0xffffffffu, f);
+            if (f) find[b + base + __popc(m & ((1u << lane) - 1u))] = x;
+            base += __popc(m);
+        }
+        if (threadIdx.x == 0)
+            row_records<OffT>(off, v, b, e, wrote, small_cap, big_chunk, item_shift, deg, fcnt,
+                              vinfo, ctr, bitem, irow);
+        __syncthreads();
     }
 }
 
@@ -1184,6 +1325,84 @@ count_rows_kernel(const OffT *__restrict__ off, const int *__restrict__ ind,
     if (lane == 0 && tri_local) atomicAdd(&ctr->tri_total, tri_local);
 }
 
+// Lane-per-row kernel for low-degree graphs with vertex-id labels, in place
+// of count_rows_kernel.  It takes the same edges: every oriented edge u -> w
+// (w in N+(u)) whose longer forward list has at most small_cap members and
+// whose shorter one is not empty -- the edges whose apex count_rows_kernel
+// would own -- and counts |N+(u) ∩ N+(w)| by merging the two lists, which are
+// in ascending id order (the forward build keeps each row's order).  A lane
+// owns a row u and all its edges, so the credits need no cross-lane work:
+// u's in a register (one atomic per row), w's per edge, and each third vertex
+// x in N+(u) in a per-lane 8-bit shared counter flushed once per (u, x)
+// (a count is at most small_cap - 1 <= 127).  Warps take 32 rows at a time
+// from a dynamic queue.  Trades the flattened warp machinery of
+// count_rows_kernel (about 200 warp instructions per row on a mean-degree-12
+// graph) for short serial merges when every list is short.
+template <bool PER_VERTEX>
+__global__ void __launch_bounds__(kRowThreads)
+merge_rows_kernel(long long n, const VInfo *__restrict__ vinfo, const int *__restrict__ find,
+                  unsigned long long *__restrict__ tacc, Counters *ctr, int small_cap)
+{
+    extern __shared__ unsigned char s_hit[];           // [small_cap][kRowThreads]
+    const int lane = threadIdx.x & 31;
+    unsigned char *hit = s_hit + threadIdx.x;
+    unsigned long long tri_local = 0;
+    while (true) {
+        unsigned long long grp = 0;
+        if (lane == 0) grp = atomicAdd(&ctr->row_items, 1ull);
+        const long long u0 = (long long)__shfl_sync(0xffffffffu, grp, 0) * 32;
+        if (u0 >= n) break;
+        const long long u = u0 + lane;
+        int fu = 0;
+        long long fb = 0;
+        if (u < n) {
+            const VInfo vi = vinfo[u];
+            fu = vi.fdeg;
+            fb = vi.fbeg;
+        }
+        if (fu > small_cap) fu = 0;                 // the block kernel's apex
+        const int *A = find + fb;
+        if (PER_VERTEX)
+            for (int i = 0; i < fu; ++i) hit[i * kRowThreads] = 0;
+        unsigned int cu = 0;
+        for (int j = 0; j < fu; ++j) {
+            const int w = A[j];
+            const VInfo vw = vinfo[w];
+            const int fw = vw.fdeg;
+            if (fw == 0 || fw > small_cap) continue;
+            const int *B = find + vw.fbeg;
+            int i = 0, k = 0;
+            int a = A[0], b = B[0];
+            unsigned int cw = 0;
+            while (true) {
+                if (a == b) {
+                    ++cw;
+                    if (PER_VERTEX) ++hit[i * kRowThreads];
+                }
+                const int ni = i + (a <= b), nk = k + (b <= a);
+                if (ni >= fu || nk >= fw) break;
+                a = A[ni];
+                b = B[nk];
+                i = ni;
+                k = nk;
+            }
+            if (PER_VERTEX && cw) atomicAdd(&tacc[w], (unsigned long long)cw);
+            cu += cw;
+        }
+        if (PER_VERTEX && cu) {
+            atomicAdd(&tacc[u], (unsigned long long)cu);
+            for (int i = 0; i < fu; ++i) {
+                const unsigned int c = hit[i * kRowThreads];
+                if (c) atomicAdd(&tacc[A[i]], (unsigned long long)c);
+            }
+        }
+        tri_local += cu;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) tri_local += __shfl_down_sync(0xffffffffu, tri_local, d);
+    if (lane == 0 && tri_local) atomicAdd(&ctr->tri_total, tri_local);
+}
+
 // Block-per-row kernel for apexes whose forward list exceeds small_cap.
 // Vertex-id labels: the whole block shares one hash table of up to
 // kBigTableSlots slots (load factor <= 1/8 up to kBigTableSlots/8 keys,
@@ -1425,6 +1644,7 @@ int g_sm_count[64];
 int g_rows_blocks[64][8];
 int g_big_blocks[64][4];
 int g_sort_blocks[64][2];
+int g_merge_blocks[64][8];
 
 int device_sm_count(int dev)
 {
@@ -1477,6 +1697,8 @@ Plan make_plan(long long n, long long nnz, int off_bits, bool per_vertex)
     p.o_irow = take(sizeof(long long) * (size_t)(div_up<long long>(nnz, kMinItemLen) + 1));
     // block-kernel items: at most one per row plus one per kMinBigChunk entries
     p.o_bitem = take(sizeof(int2) * (size_t)(n + div_up<long long>(nnz, kMinBigChunk) + 1));
+    // rows longer than kLongRowMin, at most nnz / (kLongRowMin + 1) of them
+    p.o_long = take(sizeof(int) * (size_t)(nnz / (kLongRowMin + 1) + 1));
     p.bytes = o;
     return p;
 }
@@ -1526,13 +1748,14 @@ gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
     return GTC_OK;
 }
 
-int launches_per_count(const RowConfig &cfg, bool per_vertex)
+int launches_per_count(const RowConfig &cfg, bool per_vertex, long long n)
 {
-    // vertex-id labels: row placement; rank labels: degree histogram, rank
-    // scan, rank, tile bounds, tile placement, list sort, vinfo.  Then the
-    // warp kernel, the block kernel, the global count and, per vertex,
-    // finalize.
-    return (cfg.rank_labels ? 7 : 1) + 3 + (per_vertex ? 1 : 0);
+    // vertex-id labels: row placement (and, from kRowPlaceWarpMin rows on,
+    // the long-row placement); rank labels: degree histogram, rank scan,
+    // rank, tile bounds, tile placement, list sort, vinfo.  Then the warp
+    // kernel, the block kernel, the global count and, per vertex, finalize.
+    const int build = cfg.rank_labels ? 7 : (n >= kRowPlaceWarpMin ? 2 : 1);
+    return build + 3 + (per_vertex ? 1 : 0);
 }
 
 template <typename OffT>
@@ -1611,18 +1834,37 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                                                        cfg.big_chunk, ceil_log2(cfg.item_len),
                                                        vinfo, ctr, bitem, irow);
         } else {
-            // one row per group of gs lanes, gs ~ the mean degree
+            // groups of gs lanes, gs ~ the mean degree; a group per row for
+            // small graphs, a warp per 32 rows from kRowPlaceWarpMin rows on
             const double mean = (double)nnz / (double)n;
             const int gs = mean <= 8.0 ? 8 : (mean <= 16.0 ? 16 : 32);
-            const unsigned pb = (unsigned)div_up<long long>(n * gs, 256);
-            auto place = [&](auto kern) {
-                kern<<<pb, 256, 0, stream>>>(off, ind, n, deg, fcnt, find, vinfo, small_cap,
-                                             cfg.big_chunk, ceil_log2(cfg.item_len), ctr, bitem,
-                                             irow, status);
-            };
-            if (gs == 8) place(row_place_kernel<OffT, 8>);
-            else if (gs == 16) place(row_place_kernel<OffT, 16>);
-            else place(row_place_kernel<OffT, 32>);
+            const bool per_warp = n >= kRowPlaceWarpMin;
+            const int ishift = ceil_log2(cfg.item_len);
+            int *long_rows = reinterpret_cast<int *>(base + p.o_long);
+            if (per_warp) {
+                const unsigned pb = (unsigned)div_up<long long>(n, 256);
+                auto place = [&](auto kern) {
+                    kern<<<pb, 256, 0, stream>>>(off, ind, n, deg, fcnt, find, vinfo, small_cap,
+                                                 cfg.big_chunk, ishift, ctr, bitem, irow,
+                                                 long_rows, status);
+                };
+                if (gs == 8) place(row_place_warp_kernel<OffT, 8>);
+                else if (gs == 16) place(row_place_warp_kernel<OffT, 16>);
+                else place(row_place_warp_kernel<OffT, 32>);
+                long_row_place_kernel<OffT><<<(unsigned)(device_sm_count(dev) * 4), 256, 0,
+                                              stream>>>(off, ind, n, deg, fcnt, find, vinfo,
+                                                        small_cap, cfg.big_chunk, ishift, ctr,
+                                                        bitem, irow, long_rows, status);
+            } else {
+                const unsigned pb = (unsigned)div_up<long long>(n * gs, 256);
+                auto place = [&](auto kern) {
+                    kern<<<pb, 256, 0, stream>>>(off, ind, n, deg, fcnt, find, vinfo, small_cap,
+                                                 cfg.big_chunk, ishift, ctr, bitem, irow, status);
+                };
+                if (gs == 8) place(row_place_kernel<OffT, 8>);
+                else if (gs == 16) place(row_place_kernel<OffT, 16>);
+                else place(row_place_kernel<OffT, 32>);
+            }
         }
         nvtxRangePop();
         if (timing) cudaEventRecord(timing->ev[1], stream);
@@ -1639,7 +1881,17 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                                                          status, irow, n_items, cfg.item_len,
                                                          small_cap, cfg.region_mult, lorder);
             };
-            {
+            if (cfg.merge_rows && !rank_labels) {
+                NvtxRange r("gtc: warp kernel");
+                auto kern = per_vertex ? merge_rows_kernel<true> : merge_rows_kernel<false>;
+                const size_t msmem = per_vertex ? (size_t)small_cap * kRowThreads : 0;
+                int *cache = &g_merge_blocks[dev & 63][(per_vertex ? 4 : 0) +
+                                                       (ceil_log2(cfg.group) & 3)];
+                int blocks = occupancy_blocks(kern, kRowThreads, msmem, dev, cache);
+                const long long need = div_up<long long>(n, kRowThreads);
+                if (need < blocks) blocks = (int)need;
+                kern<<<blocks, kRowThreads, msmem, stream>>>(n, vinfo, find, tacc, ctr, small_cap);
+            } else {
                 NvtxRange r("gtc: warp kernel");
                 if (per_vertex) launch_rows(count_rows_kernel<true, OffT>);
                 else launch_rows(count_rows_kernel<false, OffT>);

@@ -15,11 +15,13 @@ struct RowConfig {
     bool rank_labels = true;  // label vertices by degree rank (skewed graphs)
     int region_mult = 4;      // warp kernel: table slots per forward member (2 or 4);
                               // low-degree graphs fit twice the rows per batch with 2
+    bool merge_rows = false;  // vertex-id labels: lane-per-row merge kernel in place of
+                              // the warp-per-item kernel
 };
 
 // Kernel launches of one run_count with this configuration (the epilogue
 // kernels counted as launched).
-int launches_per_count(const RowConfig &cfg, bool per_vertex);
+int launches_per_count(const RowConfig &cfg, bool per_vertex, long long n);
 
 // Apply caller overrides (gtc_tuning, 0 = keep) to cfg; GTC_ERR_INVALID_ARGUMENT
 // for a value outside the documented ranges.

@@ -34,6 +34,8 @@ namespace gtc {
 constexpr int kPrepThreads = 256;           // merge-path tile kernels
 constexpr int kPrepItemsPerThread = 8;      // (rows + entries) per thread
 constexpr int kPrepTile = kPrepThreads * kPrepItemsPerThread;
+constexpr long long kRowPlaceWarpMin = 1ll << 18;   // rows from which a warp takes 32 rows
+constexpr int kLongRowMin = 64;             // shortest row the per-warp placement hands on
 
 constexpr int kRowThreads = 256;            // warp-per-item count kernel
 constexpr int kRowSlots = 512;              // shared table slots per warp
@@ -127,7 +129,7 @@ struct Plan {
     // workspace byte offsets
     size_t o_status = 0, o_counters = 0, o_deg = 0, o_fcnt = 0, o_vinfo = 0, o_find = 0,
            o_tacc = 0, o_trow = 0, o_irow = 0, o_hist = 0, o_rank = 0, o_order = 0,
-           o_bitem = 0;
+           o_bitem = 0, o_long = 0;
     size_t bytes = 0;
 };
 
@@ -139,7 +141,8 @@ struct Counters {
     unsigned long long big_rows;      // number of rows for the block kernel
     unsigned long long sort_groups;   // dynamic queue of 32-row groups, list sort
     unsigned long long big_total;     // block-kernel items posted by the forward build
-    unsigned long long pad[2];
+    unsigned long long long_rows;     // rows the per-warp row placement leaves to blocks
+    unsigned long long long_next;     // dynamic queue over those rows
 };
 
 

@@ -55,7 +55,7 @@ def test_workspace_size_host_only():
 def test_launch_plan_host_only():
     """Label choice and kernel count per configuration, without a device."""
     from gputrianglecounting_b200 import api
-    assert api.launch_plan(1 << 20, 12 << 20) == {"launches": 5, "labels": "vertex-id"}
+    assert api.launch_plan(1 << 20, 12 << 20) == {"launches": 6, "labels": "vertex-id"}
     assert api.launch_plan(1 << 20, 30 << 20) == {"launches": 11, "labels": "degree-rank"}
     assert api.launch_plan(1 << 20, 30 << 20, mode="oriented")["launches"] == 10
     assert api.launch_plan(1000, 1000, tuning={"labels": 2})["labels"] == "degree-rank"

@@ -36,15 +36,17 @@ def test_int32_offsets_keeps_the_graph():
 
 
 def test_launch_counts_follow_the_library_plan():
-    """5 launches per plain count with vertex-id labels, 11 with degree-rank
-    labels; a batched step adds entry starts, globalize and per-graph T and
-    drops the global-count kernel (and, with ranks, computes graph-major
-    ranks in two more launches)."""
-    assert bench.launches_per_count(1 << 22, 50 << 20) == 5           # RGG-like: ids
+    """5 launches per plain count with vertex-id labels (6 from 2^18 rows
+    on, where long rows get their own placement launch), 11 with
+    degree-rank labels; a batched step adds entry starts, globalize and
+    per-graph T and drops the global-count kernel (and, with ranks, computes
+    graph-major ranks in two more launches)."""
+    assert bench.launches_per_count(1 << 22, 50 << 20) == 6           # RGG-like: ids
+    assert bench.launches_per_count(1 << 16, 1 << 20) == 5            # small: ids
     assert bench.launches_per_count(1 << 20, 31 << 20) == 11          # R-MAT-like: ranks
     for n, nnz, lab in itertools.product((1 << 10, 1 << 20), (1 << 14, 1 << 25), (1, 2)):
         per = bench.launches_per_count(n, nnz, {"labels": lab})
-        assert per == (5 if lab == 1 else 11)
+        assert per == ((5 if n < (1 << 18) else 6) if lab == 1 else 11)
         assert bench.batch_launches(n, nnz, {"labels": lab}) == per + (2 if lab == 1 else 4)
 
 

@@ -169,6 +169,53 @@ def test_subset(cuda):
         assert np.array_equal(out.cpu().numpy(), r_ref[v])
 
 
+def _wide_hub_graph():
+    """Two hubs of degree 2,600: hub 0's neighbours spread over 2^21 + 7
+    ids (beyond the hub kernel's bitmap span, so its rows are binary
+    searched), hub 1's packed into 2,600 consecutive ids (bitmap); the
+    neighbours are joined in a path, so both hubs close many triangles, and
+    hub 0's neighbours share a few with hub 1."""
+    n = (1 << 21) + 7
+    spread = np.unique(np.linspace(2, n - 1, 2600).astype(np.int64))
+    packed = np.arange(10, 10 + 2600, dtype=np.int64)
+    edges = [(0, int(x)) for x in spread] + [(1, int(x)) for x in packed]
+    edges += [(int(a), int(b)) for a, b in zip(spread[:-1], spread[1:])]
+    edges += [(int(a), int(b)) for a, b in zip(packed[:-1:2], packed[1::2])]
+    edges += [(0, 1)]
+    return G.from_edge_list(n, sorted({(min(a, b), max(a, b)) for a, b in edges if a != b}))
+
+
+@pytest.mark.parametrize("which", ["rmat", "wide"])
+def test_subset_hub_rows(which, cuda):
+    """Listed rows longer than the hash table (the hub kernel, a whole GPU
+    per hub), listed several times and spread over several 1,024-vertex
+    scan chunks, beside ordinary rows; the int32 vertex-list shim as well."""
+    if which == "rmat":
+        g = G.rmat(16, 16, 7).numpy()
+    else:
+        g = _wide_hub_graph()
+    deg = np.diff(g.off)
+    hubs = np.nonzero(deg > 2048)[0]
+    assert hubs.size >= 2
+    rng = np.random.default_rng(3)
+    v = np.concatenate([hubs, rng.integers(0, g.n, 3000), hubs[::-1], [hubs[0]] * 3])
+    v = v[rng.permutation(v.size)].astype(np.int32)
+    ref = O.subset(g.off, g.ind, v)
+    assert ref[np.isin(v, hubs)].min() > 0
+    for off_dtype in (torch.int64, torch.int32):
+        d_off, d_ind = _dev(g.off, g.ind, cuda, off_dtype)
+        out = api.count_subset(d_off, d_ind, torch.as_tensor(v).to(cuda))
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), ref), off_dtype
+    d_off = torch.as_tensor(g.off).to(cuda, torch.int32)
+    d_ind = torch.as_tensor(g.ind).to(cuda, torch.int32)
+    d_v = torch.as_tensor(v).to(cuda)
+    vout = torch.full((v.size,), -1, dtype=torch.int32, device=cuda)
+    api.kernelCall(4, 128, v.size, d_off, d_ind, vout, 1, 128, 0, vertex=d_v)
+    torch.cuda.synchronize()
+    assert np.array_equal(vout.cpu().numpy().astype(np.int64), ref)
+
+
 def test_compat_kernelCall(cuda):
     """The reference's kernelCall argument list (src/gpurun.cu:31-37)."""
     g = G.rmat(12, 12, 6).numpy()
