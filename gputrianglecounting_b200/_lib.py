@@ -62,7 +62,8 @@ _SIGNATURES = {
 class Tuning(ctypes.Structure):
     """gtc_tuning (0 = library choice)."""
     _fields_ = [("group", c_int), ("item_len", c_int), ("big_chunk", c_int),
-                ("big_hash_max", c_int), ("labels", c_int), ("region", c_int)]
+                ("big_hash_max", c_int), ("labels", c_int), ("region", c_int),
+                ("rows", c_int)]
 
 
 _lib = None

@@ -16,13 +16,16 @@ grids in src/param.cu:2-6).  The knobs here never change a result (tested):
                id) (1) or degree ranks with rank-sorted forward lists and the
                block kernel's rank bitmap (2);
   region       warp-kernel hash slots per forward-list member (2 or 4):
-               rows per table batch against collisions.
+               rows per table batch against collisions;
+  rows         the group kernel's form with vertex-id labels: a warp per
+               work item with per-row hash regions (1) or per-row merges of
+               the id-ordered lists (2).
 
 A graph's *degree profile* -- size, mean degree and skew buckets -- keys a
 cache (in memory and, optionally, a JSON file), so each profile is tuned
 once.  Each candidate is timed with CUDA events on the device (best of a few
 runs after a warm-up).  search="grid" times every combination; "staged"
-first picks labels x group x region with the other knobs at the library's choice,
+first picks labels x group x region x rows with the other knobs at the library's choice,
 then item_len x big_chunk under that choice (for inputs whose single count
 takes long, such as a whole batch).
 """
@@ -41,11 +44,12 @@ from . import api
 DEFAULT_GRID = {
     "labels": (1, 2),
     "region": (2, 4),
+    "rows": (1, 2),
     "group": (8, 16, 32),
     "item_len": (128, 256, 512, 1024),
     "big_chunk": (1024, 2048, 4096),
 }
-STAGES = (("labels", "group", "region"), ("item_len", "big_chunk"))
+STAGES = (("labels", "group", "region", "rows"), ("item_len", "big_chunk"))
 
 _lock = threading.Lock()
 _memory: dict[str, dict] = {}
@@ -81,11 +85,22 @@ def save_cache(path: str | None, cache: dict) -> None:
     os.replace(tmp, path)
 
 
+def valid(tuning: dict) -> bool:
+    """Per-row merges need vertex-id labels and use no hash regions, so
+    (rows 2, labels 2) is rejected by the library and (rows 2, region 4)
+    would time (rows 2, region 2) again."""
+    if tuning.get("rows") == 2:
+        return tuning.get("labels") != 2 and tuning.get("region", 2) == 2
+    return True
+
+
 def candidates(grid: dict | None = None):
     grid = grid or DEFAULT_GRID
     keys = sorted(grid)
     for vals in itertools.product(*(grid[k] for k in keys)):
-        yield dict(zip(keys, vals))
+        cand = dict(zip(keys, vals))
+        if valid(cand):
+            yield cand
 
 
 def _search(time_fn, grid: dict, search: str):
@@ -104,6 +119,8 @@ def _search(time_fn, grid: dict, search: str):
             continue
         for cand in candidates(sub):
             tun = dict(best, **cand)
+            if not valid(tun):
+                continue
             ms = time_fn(tun)
             timed += 1
             if ms < best_ms:

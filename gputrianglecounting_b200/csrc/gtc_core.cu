@@ -619,11 +619,8 @@ __global__ void vinfo_kernel(const OffT *__restrict__ off, const int *__restrict
 // are written.  Two launch forms:
 //   * row_place_kernel: one group per row, its first lane writing the row's
 //     records (small graphs: the most groups in flight);
-//   * row_place_warp_kernel: a warp per 32 consecutive rows; one lane per row
-//     loads the offsets and writes the records (coalesced) and the groups
-//     take the rows in turn; rows longer than max(8 x GS, kLongRowMin) are
-//     listed for long_row_place_kernel, a block per row, so that a hub holds
-//     up neither its warp's other rows nor a single group (large graphs).
+//   * row_place_lane_kernel (below): a thread per row, from kRowPlaceWarpMin
+//     rows on (large graphs).
 template <int GS>
 __device__ __forceinline__ int place_row(const int *__restrict__ ind, const void *offp,
                                          bool off32, long long n, long long v, long long b,
@@ -694,50 +691,66 @@ row_place_kernel(const OffT *__restrict__ off, const int *__restrict__ ind, long
                           ctr, bitem, irow);
 }
 
-template <typename OffT, int GS>
+// Thread-per-row form of the forward build for large graphs: each thread
+// walks its own row serially, four entries at a time (the four id loads, then
+// the eight offset loads, issued together), appending the entries ordered
+// above the row to the start of the row's segment; rows longer than
+// kLongRowMin are listed for long_row_place_kernel, a block per row, so that
+// a hub holds up no warp.  On a 4 M-vertex mean-degree-12 graph it issues
+// 105 M warp instructions where a 16-lane group per row (rows taken in turn
+// by a warp's groups) issued 256 M, and takes 0.19 ms instead of 0.31; the
+// offsets gather sets the pace.
+template <typename OffT>
 __global__ void __launch_bounds__(256)
-row_place_warp_kernel(const OffT *__restrict__ off, const int *__restrict__ ind, long long n,
+row_place_lane_kernel(const OffT *__restrict__ off, const int *__restrict__ ind, long long n,
                       int *__restrict__ deg, int *__restrict__ fcnt, int *__restrict__ find,
                       VInfo *__restrict__ vinfo, int small_cap, int big_chunk, int item_shift,
                       Counters *ctr, int2 *__restrict__ bitem, long long *__restrict__ irow,
                       int *__restrict__ long_rows, unsigned int *status)
 {
-    constexpr int kGroups = 32 / GS;
-    constexpr int kLong = 8 * GS > kLongRowMin ? 8 * GS : kLongRowMin;   // handed on beyond
-    const int lane = threadIdx.x & 31, glane = lane % GS, gi = lane / GS;
-    const long long v0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x - lane);
-    if (v0 >= n) return;                         // uniform across the warp
-    const long long my_v = v0 + lane;
-    const bool my_ok = my_v < n;
-    const long long my_b = my_ok ? (long long)off[my_v] : 0;
-    const long long my_e = my_ok ? (long long)off[my_v + 1] : 0;
-    const bool my_long = my_e - my_b > kLong;
-    int my_wrote = 0;
-#pragma unroll 1
-    for (int it = 0; it < 32 / kGroups; ++it) {
-        const int rl = it * kGroups + gi;            // this group's row (lane index)
-        const long long v = v0 + rl;
-        const long long b = __shfl_sync(0xffffffffu, my_b, rl);
-        const long long e = __shfl_sync(0xffffffffu, my_e, rl);
-        int wrote = 0;
-        if (v < n && e - b <= kLong)
-            wrote = place_row<GS>(ind, off, sizeof(OffT) == 4, n, v, b, (int)(e - b), glane, find,
-                                  status);
-        // row rl's count goes to lane rl
-        const int got = __shfl_sync(0xffffffffu, wrote, (lane % kGroups) * GS);
-        if (lane / kGroups == it) my_wrote = got;
-    }
-    if (my_ok && my_long) {
-        // long rows go to long_row_place_kernel, a block per row
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const long long b = (long long)off[v], e = (long long)off[v + 1];
+    const int d = (int)(e - b);
+    if (d > kLongRowMin) {
         const unsigned long long at = atomicAdd(&ctr->long_rows, 1ull);
-        long_rows[at] = (int)my_v;
-    } else if (my_ok) {
-        row_records<OffT>(off, my_v, my_b, my_e, my_wrote, small_cap, big_chunk, item_shift, deg,
-                          fcnt, vinfo, ctr, bitem, irow);
+        long_rows[at] = (int)v;
+        return;
     }
+    int wrote = 0;
+    bool bad = false;
+    auto keep = [&](int x, long long dx) {
+        if (dx > d || (dx == d && x > v)) find[b + wrote++] = x;
+    };
+    int k = 0;
+    for (; k + 4 <= d; k += 4) {
+        int x[4];
+        long long dx[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) x[j] = ind[b + k + j];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const bool ok = (unsigned long long)(long long)x[j] < (unsigned long long)n;
+            bad |= !ok;
+            dx[j] = ok ? (long long)off[x[j] + 1] - (long long)off[x[j]] : -1;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (dx[j] >= 0) keep(x[j], dx[j]);
+    }
+    for (; k < d; ++k) {
+        const int x = ind[b + k];
+        if ((unsigned long long)(long long)x < (unsigned long long)n)
+            keep(x, (long long)off[x + 1] - (long long)off[x]);
+        else
+            bad = true;
+    }
+    if (bad) atomicOr(status, kErrIndexRange);
+    row_records<OffT>(off, v, b, e, wrote, small_cap, big_chunk, item_shift, deg, fcnt, vinfo, ctr,
+                      bitem, irow);
 }
 
-// The rows row_place_warp_kernel handed on (longer than its limit), a block
+// The rows row_place_lane_kernel handed on (longer than kLongRowMin), a block
 // per row from a dynamic queue: the block's warps each take a contiguous
 // slice of the row, count their forward entries, place them after the
 // earlier slices' (a block scan of the counts), and the row's records follow.
@@ -1716,6 +1729,10 @@ RowConfig pick_row_config(long long n, long long nnz)
     // small graphs: shorter warp items, so that there are enough to fill
     // every SM (an ER graph of 16,384 vertices counts 17% faster)
     if (nnz < (4ll << 20)) c.item_len = 128;
+    // large graphs with vertex-id labels: per-row merges (a 4 M-vertex
+    // mean-degree-12 graph's group kernel takes 0.87 ms instead of 0.97; a
+    // 16 K-vertex ER graph's 0.062 instead of 0.037, hence the bound)
+    c.merge_rows = !c.rank_labels && n >= kRowPlaceWarpMin;
     return c;
 }
 
@@ -1737,7 +1754,9 @@ gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
         tuning->big_hash_max < 0 ||
         tuning->big_hash_max > kBigHashMaxFdeg || tuning->big_chunk > 32768 ||
         tuning->labels < 0 || tuning->labels > 2 ||
-        (tuning->region != 0 && tuning->region != 2 && tuning->region != 4))
+        (tuning->region != 0 && tuning->region != 2 && tuning->region != 4) ||
+        tuning->rows < 0 || tuning->rows > 2 ||
+        (tuning->rows == GTC_ROWS_MERGE && tuning->labels == GTC_LABELS_DEGREE_RANK))
         return GTC_ERR_INVALID_ARGUMENT;
     if (tuning->item_len) cfg.item_len = tuning->item_len;
     if (tuning->big_chunk) cfg.big_chunk = tuning->big_chunk;
@@ -1745,6 +1764,13 @@ gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
     if (tuning->labels == GTC_LABELS_VERTEX_ID) cfg.rank_labels = false;
     if (tuning->labels == GTC_LABELS_DEGREE_RANK) cfg.rank_labels = true;
     if (tuning->region) cfg.region_mult = tuning->region;
+    if (tuning->rows == GTC_ROWS_HASH) cfg.merge_rows = false;
+    if (tuning->rows == GTC_ROWS_MERGE) {
+        cfg.merge_rows = true;
+        cfg.rank_labels = false;
+    }
+    // the merge kernel needs id-ordered lists
+    if (cfg.rank_labels) cfg.merge_rows = false;
     return GTC_OK;
 }
 
@@ -1834,23 +1860,18 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                                                        cfg.big_chunk, ceil_log2(cfg.item_len),
                                                        vinfo, ctr, bitem, irow);
         } else {
-            // groups of gs lanes, gs ~ the mean degree; a group per row for
-            // small graphs, a warp per 32 rows from kRowPlaceWarpMin rows on
+            // small graphs: a group of gs lanes (about the mean degree) per
+            // row; from kRowPlaceWarpMin rows on a thread per row, the long
+            // rows a block each
             const double mean = (double)nnz / (double)n;
             const int gs = mean <= 8.0 ? 8 : (mean <= 16.0 ? 16 : 32);
-            const bool per_warp = n >= kRowPlaceWarpMin;
             const int ishift = ceil_log2(cfg.item_len);
             int *long_rows = reinterpret_cast<int *>(base + p.o_long);
-            if (per_warp) {
-                const unsigned pb = (unsigned)div_up<long long>(n, 256);
-                auto place = [&](auto kern) {
-                    kern<<<pb, 256, 0, stream>>>(off, ind, n, deg, fcnt, find, vinfo, small_cap,
-                                                 cfg.big_chunk, ishift, ctr, bitem, irow,
-                                                 long_rows, status);
-                };
-                if (gs == 8) place(row_place_warp_kernel<OffT, 8>);
-                else if (gs == 16) place(row_place_warp_kernel<OffT, 16>);
-                else place(row_place_warp_kernel<OffT, 32>);
+            if (n >= kRowPlaceWarpMin) {
+                row_place_lane_kernel<OffT><<<(unsigned)div_up<long long>(n, 256), 256, 0,
+                                              stream>>>(off, ind, n, deg, fcnt, find, vinfo,
+                                                        small_cap, cfg.big_chunk, ishift, ctr,
+                                                        bitem, irow, long_rows, status);
                 long_row_place_kernel<OffT><<<(unsigned)(device_sm_count(dev) * 4), 256, 0,
                                               stream>>>(off, ind, n, deg, fcnt, find, vinfo,
                                                         small_cap, cfg.big_chunk, ishift, ctr,

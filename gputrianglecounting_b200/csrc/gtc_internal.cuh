@@ -34,8 +34,8 @@ namespace gtc {
 constexpr int kPrepThreads = 256;           // merge-path tile kernels
 constexpr int kPrepItemsPerThread = 8;      // (rows + entries) per thread
 constexpr int kPrepTile = kPrepThreads * kPrepItemsPerThread;
-constexpr long long kRowPlaceWarpMin = 1ll << 18;   // rows from which a warp takes 32 rows
-constexpr int kLongRowMin = 64;             // shortest row the per-warp placement hands on
+constexpr long long kRowPlaceWarpMin = 1ll << 18;   // rows from which a thread takes a row
+constexpr int kLongRowMin = 64;             // longest row a placement thread takes
 
 constexpr int kRowThreads = 256;            // warp-per-item count kernel
 constexpr int kRowSlots = 512;              // shared table slots per warp

@@ -129,6 +129,12 @@ gtc_status gtc_count_status(const void *d_workspace, size_t ws_bytes,
  *                bitmap); the library picks ranks for mean degree > 24
  *   region       warp-kernel hash slots per forward-list member: 2 or 4 (the
  *                library picks 2 for mean degree <= 24, else 4)
+ *   rows         the group kernel's form: 1 = warp per work item with per-row
+ *                hash regions, 2 = per-row merges of id-ordered forward lists
+ *                (vertex-id labels only; with labels = 2 it is rejected, with
+ *                labels = 0 it implies vertex ids).  The library picks 2 for
+ *                single graphs with vertex-id labels and at least 2^18
+ *                vertices, else 1
  */
 typedef struct gtc_tuning {
     int group;
@@ -137,10 +143,13 @@ typedef struct gtc_tuning {
     int big_hash_max;
     int labels;
     int region;
+    int rows;
 } gtc_tuning;
 
 /* Values of gtc_tuning.labels. */
 enum { GTC_LABELS_AUTO = 0, GTC_LABELS_VERTEX_ID = 1, GTC_LABELS_DEGREE_RANK = 2 };
+/* Values of gtc_tuning.rows. */
+enum { GTC_ROWS_AUTO = 0, GTC_ROWS_HASH = 1, GTC_ROWS_MERGE = 2 };
 
 /*
  * What gtc_count_tuned would run for this graph size and tuning (NULL = the

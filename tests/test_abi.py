@@ -99,6 +99,13 @@ def test_invalid_arguments_rejected_before_any_device_work():
     for bad_len in (65536, 65535, 48, 100):
         with pytest.raises(_lib.GTCError):
             api.launch_plan(1000, 90000, tuning={"item_len": bad_len})
+    # the merge form of the group kernel needs vertex-id labels: rejected with
+    # rank labels, implies vertex ids with automatic labels
+    for bad_tun in ({"rows": 3}, {"rows": -1}, {"rows": 2, "labels": 2}):
+        with pytest.raises(_lib.GTCError):
+            api.launch_plan(1000, 90000, tuning=bad_tun)
+    assert api.launch_plan(1 << 20, 30 << 20, tuning={"rows": 2})["labels"] == "vertex-id"
+    assert api.launch_plan(1 << 20, 30 << 20, tuning={"rows": 1})["labels"] == "degree-rank"
     # status query needs a workspace
     assert lib.gtc_count_status(None, 256, None, None) == 1
     assert lib.gtc_count_status(fake, 2, None, None) == 1

@@ -19,19 +19,26 @@ def test_profile_buckets_and_cache_roundtrip(tmp_path):
     path = str(tmp_path / "tune.json")
     autotune.save_cache(path, {"plain:x": {"tuning": {"group": 8}, "ms": 1.0}})
     assert autotune.load_cache(path)["plain:x"]["tuning"] == {"group": 8}
-    assert len(list(autotune.candidates())) == 144
+    # 2 x 2 x 2 x 3 x 4 x 3 combinations less the 72 with merges under rank
+    # labels and the 36 with merges and 4 hash slots per member
+    assert len(list(autotune.candidates())) == 180
+    assert not autotune.valid({"rows": 2, "labels": 2})
+    assert not autotune.valid({"rows": 2, "labels": 1, "region": 4})
+    assert autotune.valid({"rows": 2, "labels": 1, "region": 2}) and autotune.valid({"rows": 1})
 
 
 def test_staged_search_host_only():
-    """Staged search: labels x group x region first (other knobs at the
+    """Staged search: labels x group x region x rows first (other knobs at the
     library's choice), then item_len x big_chunk under the winner."""
     cost = lambda t: (abs(t.get("group", 32) - 16) + (0 if t.get("labels") == 2 else 5)
                       + abs(t.get("item_len", 512) - 256) / 100 + t.get("big_chunk", 2048) / 1e4)
     ms, best, timed = autotune._search(cost, autotune.DEFAULT_GRID, "staged")
-    assert best == {"labels": 2, "group": 16, "region": 2, "item_len": 256, "big_chunk": 1024}
-    assert timed == 2 * 3 * 2 + 4 * 3
+    assert best == {"labels": 2, "group": 16, "region": 2, "rows": 1, "item_len": 256,
+                    "big_chunk": 1024}
+    # stage 1: 3 groups x (ids: 2 regions x hash + merge; ranks: 2 regions)
+    assert timed == 3 * (3 + 2) + 4 * 3
     ms_g, best_g, timed_g = autotune._search(cost, autotune.DEFAULT_GRID, "grid")
-    assert best_g == best and timed_g == 144
+    assert best_g == best and timed_g == 180
     with pytest.raises(ValueError):
         autotune._search(cost, autotune.DEFAULT_GRID, "random")
 

@@ -39,7 +39,7 @@ def test_batch_matches_oracle_and_single_graph(cuda):
     bc = api.BatchCounter(cuda)
     for tun in (None, {"group": 4}, {"group": 32, "item_len": 64, "big_chunk": 64},
                 {"labels": 2}, {"labels": 2, "group": 4, "big_chunk": 64},
-                {"labels": 1, "group": 4, "big_hash_max": 8}):
+                {"labels": 1, "group": 4, "big_hash_max": 8}, {"rows": 2, "group": 16}):
         res = bc.count(batch, outputs=("r", "lcc", "graph_T"), tuning=tun)
         torch.cuda.synchronize()
         _check_against_oracle(graphs, batch, res)

@@ -18,8 +18,10 @@ _SHAPES = [{}, {"group": 4}, {"group": 8}, {"group": 16, "region": 2}, {"group":
            {"group": 4, "big_hash_max": 8},     # block kernel's in-place search path
            {"group": 32, "item_len": 32, "big_chunk": 32, "big_hash_max": 16}]
 # every launch shape with vertex-id labels (1) and degree-rank labels (2),
-# plus the library's own choice
-TUNINGS = [None] + [dict(t, labels=lab) for t in _SHAPES for lab in (1, 2)]
+# the group kernel's merge form (rows 2, vertex ids implied) under the shapes
+# that set the group, plus the library's own choice
+TUNINGS = ([None] + [dict(t, labels=lab) for t in _SHAPES for lab in (1, 2)]
+           + [dict(t, rows=2) for t in _SHAPES if "group" in t])
 
 
 def _dev(off, ind, dev, off_dtype=torch.int64):

@@ -31,11 +31,13 @@ with open(os.path.join(HERE, "golden", "fullsize_digests.json")) as _f:
 
 MAKERS = {"rmat20": lambda: G.rmat(20, 16, 2), "rgg4m": lambda: G.rgg2d(1 << 22, 12, 3)}
 
-# the library's own choice, both labelings, and launch shapes that move work
-# between the warp and block kernels and through the block kernel's lookups
+# the library's own choice, both labelings, both forms of the group kernel
+# (per-row hash regions and per-row merges), and launch shapes that move work
+# between the group and block kernels and through the block kernel's lookups
 TUNINGS = [None, {"labels": 1}, {"labels": 2}, {"labels": 2, "group": 8},
            {"labels": 2, "group": 4, "big_chunk": 512, "item_len": 64},
-           {"labels": 1, "group": 16, "big_hash_max": 64}]
+           {"labels": 1, "group": 16, "big_hash_max": 64},
+           {"labels": 1, "rows": 1}, {"rows": 2, "group": 32}]
 
 
 def _sha(a: np.ndarray, dtype: str) -> str:
