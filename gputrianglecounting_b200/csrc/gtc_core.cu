@@ -19,10 +19,27 @@ namespace gtc {
 
 // ======================================================= forward-list build
 
-__device__ __forceinline__ int rank_bucket(int d)
+__host__ __device__ constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v >> 1); }
+
+// Monotone map of a degree onto B buckets (B a power of two >= 64): exact
+// below B/2, then B/32 buckets per octave -- a float with log2(B/32)
+// mantissa bits -- for the next 16 octaves, the rest in the last bucket.
+// Degrees that share a bucket above B/2 differ by less than a factor
+// 2^(32/B), so the hubs of a skewed graph stay in degree order (a linear map
+// put every degree >= B-1 into one bucket, in arbitrary order, which left the
+// largest hubs' forward lists long).
+template <int B>
+__device__ __forceinline__ int degree_bucket(int d)
 {
-    return d < 0 ? 0 : (d < kRankBuckets ? d : kRankBuckets - 1);
+    constexpr int kExact = B / 2, kPer = B / 32;
+    constexpr int kLe = ilog2(kExact), kMb = ilog2(kPer);
+    if (d < kExact) return d < 0 ? 0 : d;
+    const int l = 31 - __clz(d);
+    const int b = kExact + (l - kLe) * kPer + ((d >> (l - kMb)) & (kPer - 1));
+    return b < B ? b : B - 1;
 }
+
+__device__ __forceinline__ int rank_bucket(int d) { return degree_bucket<kRankBuckets>(d); }
 
 // Degree of vertex v (0 past the end).
 __device__ __forceinline__ int vertex_degree(const void *off_v, int off_bits, long long n,
@@ -155,7 +172,7 @@ __device__ __forceinline__ long long seg_of(const long long *__restrict__ vstart
 __device__ __forceinline__ long long seg_key(const long long *__restrict__ vstart, long long G,
                                              long long v, int d)
 {
-    return seg_of(vstart, G, v) * kSegBuckets + (d < kSegBuckets ? d : kSegBuckets - 1);
+    return seg_of(vstart, G, v) * kSegBuckets + degree_bucket<kSegBuckets>(d);
 }
 
 // deg[v] and the per-graph degree-bucket histogram ghist[g * kSegBuckets + b]
@@ -192,7 +209,7 @@ __global__ void seg_rank_kernel(const int *__restrict__ deg, long long n,
     if (v < n) {
         const long long g = seg_of(vstart, G, v);
         const int d = deg[v];
-        key = g * kSegBuckets + (d < kSegBuckets ? d : kSegBuckets - 1);
+        key = g * kSegBuckets + degree_bucket<kSegBuckets>(d);
         rank_end[v] = (int)vstart[g + 1];    // the graph's ranks end where its vertices do
     }
     const unsigned int peers = __match_any_sync(0xffffffffu, key);

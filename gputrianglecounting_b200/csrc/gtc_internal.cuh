@@ -50,9 +50,9 @@ constexpr int kBigTableSlots = 1 << kBigTableLog2;   // shared hash slots (block
 constexpr int kBigHashMaxFdeg = 2048;       // longest list hashed (load <= 1/2)
 
 // Degree-rank labels (skewed graphs): vertices are ordered by degree (a
-// counting sort over kRankBuckets degree buckets; degrees above the last
-// bucket share it) and every forward list holds the ranks of its members,
-// sorted ascending.
+// counting sort over kRankBuckets degree buckets: exact degrees below half of
+// them, then a float-like map with kRankBuckets / 32 buckets per octave) and
+// every forward list holds the ranks of its members, sorted ascending.
 constexpr int kRankBuckets = 1 << 13;
 constexpr int kRankScanThreads = 1024;
 constexpr int kRankThreads = 256;           // histogram / rank kernels
@@ -60,7 +60,7 @@ constexpr int kRankChunk = 4096;            // vertices per histogram / rank blo
 constexpr int kSortThreads = 256;           // forward-list sort kernel (warp per 32 rows)
 constexpr int kSortRegMax = 1024;           // longest list sorted in registers
 constexpr int kDirectRanks = 12288;         // block kernel: one 16-bit counter per rank
-constexpr int kTrimLoads = 4;               // block kernel: loads in flight per partner window
+constexpr int kTrimLoads = 2;               // block kernel: loads in flight per partner window
 constexpr int kBitWords = 2048;             // block kernel rank bitmap: 65536 ranks
 constexpr int kBitKeys = 2048;              // longest apex list on the bitmap path
 constexpr int kSegBuckets = 1024;           // degree buckets per graph (batched rank labels)
