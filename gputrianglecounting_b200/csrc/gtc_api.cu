@@ -263,14 +263,23 @@ subset_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
                 const long long ub = off[u], ue = off[u + 1], du = ue - ub;
                 if (u == v || du < 2) continue;
                 if (du <= 4 * dv) {
-                    for (long long i = lane; i < du; i += 32) {
-                        const long long w = (long long)ind[ub + i];
-                        unsigned int slot = hash_slot((int)w, log2t);
-                        while (true) {
-                            const long long kk = s_keys[slot];
-                            if (kk == w) { ++acc; break; }
-                            if (kk == -1) break;
-                            slot = (slot + 1) & mask;
+                    for (long long i0 = lane; i0 < du; i0 += 128) {
+                        long long wv[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const long long i = i0 + 32 * j;
+                            wv[j] = i < du ? (long long)ind[ub + i] : -1;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            if (wv[j] < 0) continue;
+                            unsigned int slot = hash_slot((int)wv[j], log2t);
+                            while (true) {
+                                const long long kk = s_keys[slot];
+                                if (kk == wv[j]) { ++acc; break; }
+                                if (kk == -1) break;
+                                slot = (slot + 1) & mask;
+                            }
                         }
                     }
                 } else {

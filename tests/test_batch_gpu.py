@@ -43,6 +43,15 @@ def test_batch_matches_oracle_and_single_graph(cuda):
         res = bc.count(batch, outputs=("r", "lcc", "graph_T"), tuning=tun)
         torch.cuda.synchronize()
         _check_against_oracle(graphs, batch, res)
+    # adjacency at an address that is not 16-byte aligned: the id
+    # globalization takes its scalar path, with the same result
+    shifted = torch.empty(batch.ind.numel() + 1, dtype=torch.int32, device=cuda)
+    shifted[1:] = batch.ind
+    unaligned = api.BatchCSR(batch.vstart, batch.off, shifted[1:])
+    assert unaligned.ind.data_ptr() % 16 != 0
+    res = bc.count(unaligned, outputs=("r", "lcc", "graph_T"))
+    torch.cuda.synchronize()
+    _check_against_oracle(graphs, batch, res)
     # against single-graph gtc_count on each graph
     tc = api.TriangleCounter(cuda)
     res = bc.count(batch, outputs=("r", "graph_T"))
