@@ -587,7 +587,8 @@ sort_lists_kernel(const OffT *__restrict__ off, const int *__restrict__ fcnt, lo
 // that neither kernel starts an item with a search:
 //   * block-kernel items: a row whose forward list exceeds the warp kernel's
 //     table gets ceil(deg / big_chunk) items (row, chunk), at positions taken
-//     from one atomic counter (their order does not matter);
+//     from one atomic counter, one add per group of converged lanes (their
+//     order does not matter; a batch posts about a million such rows);
 //   * warp-kernel items: item k covers entries [k*item_len, (k+1)*item_len);
 //     the row holding entry k*item_len records itself as the item's first row.
 template <typename OffT>
@@ -599,7 +600,15 @@ __device__ __forceinline__ void post_row_items(long long v, long long b, long lo
 {
     if (fdeg > small_cap) {
         const int k = (int)div_up<long long>(d, big_chunk);
-        const unsigned long long at = atomicAdd(&ctr->big_total, (unsigned long long)k);
+        // one atomic per group of converged lanes that post items
+        auto grp = cg::coalesced_threads();
+        const int incl = cg::inclusive_scan(grp, k);
+        const int last = (int)grp.size() - 1;
+        unsigned long long base = 0;
+        if ((int)grp.thread_rank() == last)
+            base = atomicAdd(&ctr->big_total, (unsigned long long)incl);
+        base = grp.shfl(base, last);
+        const unsigned long long at = base + (unsigned long long)(incl - k);
         for (int c = 0; c < k; ++c) bitem[at + c] = make_int2((int)v, c);
     }
     // items whose first entry lies in [b, e) (item_len = 2^item_shift)
