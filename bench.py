@@ -64,8 +64,7 @@ CONFIGS = {
 # DRAM bytes (read + write) of one complete count, summed over its launches
 # from one ncu capture of the same workload (dram__bytes_read.sum +
 # dram__bytes_write.sum, cold L2 before each launch), read from the committed
-# summary profiles/dram_per_kernel_<workload>.md (its "traffic per count:"
-# line).  Far below B_alg: the forward lists and the per-vertex records stay
+# per-workload ncu summary under profiles/ (its "traffic per count:" line).  Far below B_alg: the forward lists and the per-vertex records stay
 # in the 126 MB L2, so most probe reads never reach HBM.
 def dram_traffic(workload: str) -> dict | None:
     path = os.path.join(ROOT, "profiles", f"dram_per_kernel_{workload}.md")
