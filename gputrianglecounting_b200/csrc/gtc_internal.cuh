@@ -12,9 +12,10 @@
 //      with the longer forward list (ties to the source), except that with
 //      rank labels a block-kernel apex owns every edge to a lower-ranked
 //      neighbour.  The apex's N+ is staged in shared memory (hash table, rank
-//      bitmap or per-rank counters) and the partner's N+ is probed into it,
-//      so each triangle {u,v,w} is found exactly once, at the edge between
-//      its two lowest-ordered vertices;
+//      bitmap or per-rank counters) and the partner's N+ is probed into it --
+//      or, for short lists with vertex-id labels, the two id-ordered lists
+//      are merged by one lane -- so each triangle {u,v,w} is found exactly
+//      once, at the edge between its two lowest-ordered vertices;
 //   3. credit the triangle to all three vertices: the apex through a register
 //      or block count, the partner through a warp reduction or a ballot
 //      popcount, the third vertex w through a shared per-member hit counter
