@@ -214,8 +214,11 @@ __device__ __forceinline__ void add_out(int *o, unsigned long long x)
 //   * subset_hub_kernel, all blocks on every longer ("hub") row: each block
 //     sets N(v) in a shared bitmap over the row's id span and takes every
 //     gridDim.x-th neighbour, whose row its warps probe into the bitmap with
-//     coalesced loads; block sums are added to out[k].  A row whose span
-//     exceeds the bitmap falls back to the binary search.
+//     coalesced loads; neighbour rows longer than 2,048 entries are queued
+//     and swept afterwards by all of the block's warps in 1,024-entry pieces,
+//     so that no warp is left alone with a hub's row; block sums are added to
+//     out[k].  A row whose span exceeds the bitmap falls back to the binary
+//     search.
 // Spreading a hub over the whole GPU matters: on a power-law graph a single
 // hub's probes outnumber those of thousands of ordinary rows.
 template <typename OffT, typename IndT, typename VtxT, typename OutT>
@@ -306,6 +309,9 @@ subset_hub_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
     __shared__ int s_nhub;
     __shared__ long long s_lo, s_hi;
     __shared__ unsigned long long s_sum;
+    constexpr int kBigRows = 64, kSplit = 2048, kPiece = 1024;
+    __shared__ long long s_big_b[kBigRows], s_big_e[kBigRows];
+    __shared__ int s_nbig;
     auto block = cg::this_thread_block();
     auto warp = cg::tiled_partition<32>(block);
     const int wid = warp.meta_group_rank(), lane = warp.thread_rank();
@@ -338,7 +344,7 @@ subset_hub_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
             }
             lo = cg::reduce(warp, lo, cg::less<long long>());
             hi = cg::reduce(warp, hi, cg::greater<long long>());
-            if (threadIdx.x == 0) { s_lo = LLONG_MAX; s_hi = LLONG_MIN; s_sum = 0; }
+            if (threadIdx.x == 0) { s_lo = LLONG_MAX; s_hi = LLONG_MIN; s_sum = 0; s_nbig = 0; }
             __syncthreads();
             if (lane == 0) { atomicMin(&s_lo, lo); atomicMax(&s_hi, hi); }
             __syncthreads();
@@ -357,10 +363,35 @@ subset_hub_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
                 __syncthreads();
             }
             unsigned long long acc = 0;
+            auto sweep = [&](long long b0, long long b1) {
+                // four loads in flight per lane
+                for (long long i0 = b0; i0 < b1; i0 += 128) {
+                    long long x[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const long long i = i0 + j * 32 + lane;
+                        x[j] = i < b1 ? (long long)ind[i] - lo : -1;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if ((unsigned long long)x[j] < span)
+                            acc += (s_bits[x[j] >> 5] >> (x[j] & 31)) & 1u;
+                }
+            };
             for (long long e = vb + blockIdx.x + (long long)gridDim.x * wid; e < ve; e += stride) {
                 const long long u = (long long)ind[e];
                 const long long ub = off[u], ue = off[u + 1], du = ue - ub;
                 if (u == v || du < 2) continue;
+                if (use_bits && du > kSplit) {
+                    // a long row is shared by the block's warps after this loop
+                    int at = 0;
+                    if (lane == 0) at = atomicAdd(&s_nbig, 1);
+                    at = warp.shfl(at, 0);
+                    if (at < kBigRows) {
+                        if (lane == 0) { s_big_b[at] = ub; s_big_e[at] = ue; }
+                        continue;
+                    }
+                }
                 if (use_bits) {
                     // four loads in flight per lane
                     for (long long i0 = ub; i0 < ue; i0 += 128) {
@@ -377,6 +408,16 @@ subset_hub_kernel(const OffT *__restrict__ off, const IndT *__restrict__ ind,
                     }
                 } else {
                     acc += search_shorter(ind, vb, dv, ub, du, lane);
+                }
+            }
+            if (use_bits) {
+                __syncthreads();
+                const int nbig = min(s_nbig, kBigRows);
+                for (int r = 0; r < nbig; ++r) {
+                    const long long b0 = s_big_b[r], b1 = s_big_e[r];
+                    for (long long c0 = b0 + (long long)wid * kPiece; c0 < b1;
+                         c0 += (long long)nwarps * kPiece)
+                        sweep(c0, c0 + kPiece < b1 ? c0 + kPiece : b1);
                 }
             }
             const unsigned long long ws = cg::reduce(warp, acc, cg::plus<unsigned long long>());
