@@ -218,9 +218,12 @@ def test_subset_hub_rows(which, cuda):
     assert np.array_equal(vout.cpu().numpy().astype(np.int64), ref)
 
 
-def test_compat_kernelCall(cuda):
-    """The reference's kernelCall argument list (src/gpurun.cu:31-37)."""
-    g = G.rmat(12, 12, 6).numpy()
+@pytest.mark.parametrize("which", ["rmat", "er"])
+def test_compat_kernelCall(which, cuda):
+    """The reference's kernelCall argument list (src/gpurun.cu:31-37).  The
+    R-MAT graph has a low mean degree but a high skew (the shims switch it to
+    degree-rank labels); the ER graph keeps vertex-id labels."""
+    g = (G.rmat(12, 12, 6) if which == "rmat" else G.erdos_renyi(3000, 10, 4)).numpy()
     r_ref, _, _, _ = O.per_vertex(g.off, g.ind)
     for dt in (torch.int64, torch.int32):
         d_off = torch.as_tensor(g.off).to(cuda, dt)
