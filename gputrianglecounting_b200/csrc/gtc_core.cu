@@ -645,7 +645,7 @@ __global__ void vinfo_kernel(const OffT *__restrict__ off, const int *__restrict
 // are written.  Two launch forms:
 //   * row_place_kernel: one group per row, its first lane writing the row's
 //     records (small graphs: the most groups in flight);
-//   * row_place_lane_kernel (below): a thread per row, from kRowPlaceWarpMin
+//   * row_place_lane_kernel (below): a thread per row, from kRowPlaceThreadMin
 //     rows on (large graphs).
 template <int GS>
 __device__ __forceinline__ int place_row(const int *__restrict__ ind, const void *offp,
@@ -1758,7 +1758,7 @@ RowConfig pick_row_config(long long n, long long nnz)
     // large graphs with vertex-id labels: per-row merges (a 4 M-vertex
     // mean-degree-12 graph's group kernel takes 0.87 ms instead of 0.97; a
     // 16 K-vertex ER graph's 0.062 instead of 0.037, hence the bound)
-    c.merge_rows = !c.rank_labels && n >= kRowPlaceWarpMin;
+    c.merge_rows = !c.rank_labels && n >= kRowPlaceThreadMin;
     return c;
 }
 
@@ -1802,11 +1802,11 @@ gtc_status apply_tuning(RowConfig &cfg, const gtc_tuning *tuning)
 
 int launches_per_count(const RowConfig &cfg, bool per_vertex, long long n)
 {
-    // vertex-id labels: row placement (and, from kRowPlaceWarpMin rows on,
+    // vertex-id labels: row placement (and, from kRowPlaceThreadMin rows on,
     // the long-row placement); rank labels: degree histogram, rank scan,
     // rank, tile bounds, tile placement, list sort, vinfo.  Then the warp
     // kernel, the block kernel, the global count and, per vertex, finalize.
-    const int build = cfg.rank_labels ? 7 : (n >= kRowPlaceWarpMin ? 2 : 1);
+    const int build = cfg.rank_labels ? 7 : (n >= kRowPlaceThreadMin ? 2 : 1);
     return build + 3 + (per_vertex ? 1 : 0);
 }
 
@@ -1887,13 +1887,13 @@ gtc_status run_count(const OffT *off, const int *ind, long long n, long long nnz
                                                        vinfo, ctr, bitem, irow);
         } else {
             // small graphs: a group of gs lanes (about the mean degree) per
-            // row; from kRowPlaceWarpMin rows on a thread per row, the long
+            // row; from kRowPlaceThreadMin rows on a thread per row, the long
             // rows a block each
             const double mean = (double)nnz / (double)n;
             const int gs = mean <= 8.0 ? 8 : (mean <= 16.0 ? 16 : 32);
             const int ishift = ceil_log2(cfg.item_len);
             int *long_rows = reinterpret_cast<int *>(base + p.o_long);
-            if (n >= kRowPlaceWarpMin) {
+            if (n >= kRowPlaceThreadMin) {
                 row_place_lane_kernel<OffT><<<(unsigned)div_up<long long>(n, 256), 256, 0,
                                               stream>>>(off, ind, n, deg, fcnt, find, vinfo,
                                                         small_cap, cfg.big_chunk, ishift, ctr,

@@ -35,7 +35,7 @@ namespace gtc {
 constexpr int kPrepThreads = 256;           // merge-path tile kernels
 constexpr int kPrepItemsPerThread = 8;      // (rows + entries) per thread
 constexpr int kPrepTile = kPrepThreads * kPrepItemsPerThread;
-constexpr long long kRowPlaceWarpMin = 1ll << 18;   // rows from which a thread takes a row
+constexpr long long kRowPlaceThreadMin = 1ll << 18;   // rows from which a thread takes a row
 constexpr int kLongRowMin = 64;             // longest row a placement thread takes
 
 constexpr int kRowThreads = 256;            // warp-per-item count kernel
