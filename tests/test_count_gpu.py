@@ -171,6 +171,59 @@ def test_subset(cuda):
         assert np.array_equal(out.cpu().numpy(), r_ref[v])
 
 
+def _placement_boundary_graph():
+    """2^18 + 7 vertices (the thread-per-row build's size): a ring with
+    chords (degree 4, many triangles) plus centres of degree 31-34, 62-66,
+    127-130 and 5,000 joined to runs of consecutive ring vertices (so each
+    centre closes a triangle with every consecutive pair), and fan vertices
+    with 31-33, 63-65 and 127-129 forward neighbours in a hub clique.  Rows
+    straddle the 64-entry limit of the thread-per-row build, and forward
+    lists straddle the group kernels' caps (32, 64, 128), in both
+    labelings."""
+    n = (1 << 18) + 7
+    i = torch.arange(n, dtype=torch.int64)
+    src = [i, i]
+    dst = [(i + 1) % n, (i + 2) % n]
+    # each centre is also a ring vertex (degree 4): d + 4 = 31-34, 62-66, ...
+    degs = [27, 28, 29, 30, 58, 59, 60, 61, 62, 123, 124, 125, 126, 4996]
+    for k, d in enumerate(degs):
+        c = 20 + k
+        start = 1000 + k * 9000
+        nb = torch.arange(start, start + d, dtype=torch.int64)
+        src.append(torch.full((d,), c, dtype=torch.int64))
+        dst.append(nb)
+    # a 200-vertex clique of hubs, and "fan" vertices joined to k of the hubs
+    # (all of higher degree), so that their forward lists hold exactly k
+    # members around the caps, each closing C(k, 2) triangles
+    hubs = torch.arange(200_000, 200_200, dtype=torch.int64)
+    hi, hj = torch.triu_indices(200, 200, offset=1)
+    src.append(hubs[hi])
+    dst.append(hubs[hj])
+    for k, f in enumerate([31, 32, 33, 63, 64, 65, 127, 128, 129]):
+        fan = 150_000 + 10 * k
+        src.append(torch.full((f,), fan, dtype=torch.int64))
+        dst.append(hubs[(torch.arange(f) * 7 + k) % 200])
+    return G.csr_from_pairs(torch.cat(src), torch.cat(dst), n).numpy()
+
+
+@pytest.mark.parametrize("tun", [None, {"labels": 1, "rows": 1}, {"labels": 1, "rows": 2},
+                                 {"labels": 1, "rows": 2, "group": 16},
+                                 {"labels": 1, "rows": 2, "group": 32}, {"labels": 2},
+                                 {"labels": 2, "group": 8}])
+def test_placement_and_cap_boundaries(tun, cuda):
+    g = _placement_boundary_graph()
+    deg = np.diff(g.off)
+    assert {63, 64, 65, 5000} <= set(deg.tolist())
+    r_ref, t_ref, lcc_ref, total = O.per_vertex(g.off, g.ind)
+    for off_dtype in (torch.int32, torch.int64):
+        d_off, d_ind = _dev(g.off, g.ind, cuda, off_dtype)
+        res = api.TriangleCounter(cuda).count(d_off, d_ind, tuning=tun)
+        torch.cuda.synchronize()
+        assert np.array_equal(res.r.cpu().numpy(), r_ref), (tun, off_dtype)
+        assert np.array_equal(res.lcc.cpu().numpy().view(np.int64), lcc_ref.view(np.int64))
+        assert res.total == total
+
+
 def _wide_hub_graph():
     """Two hubs of degree 2,600: hub 0's neighbours spread over 2^21 + 7
     ids (beyond the hub kernel's bitmap span, so its rows are binary
